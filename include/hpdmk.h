@@ -1,0 +1,189 @@
+/*
+ * hpdmk.h — drop-in C interface of the B200 periodic DMK energy library.
+ *
+ * Mirrors the reference's include/hpdmk.h (PDMK4MC): the same enum
+ * hpdmk_init (include/hpdmk.h:6-9), struct HPDMKParams with the same fields,
+ * defaults and layout (include/hpdmk.h:11-17), the opaque handle hpdmk_tree
+ * (include/hpdmk.h:19) and hpdmk_tree_create with the same signature
+ * (include/hpdmk.h:25). The handle-based calls below expose what the
+ * reference's C++ class HPDMKPtTree<double> offers (include/tree.hpp:74-132):
+ * construction from positions and charges, form_outgoing_pw,
+ * form_incoming_pw, eval_energy, eval_shift_energy and update_shift.
+ *
+ * Units and conventions follow the reference: positions are xyz-interleaved
+ * in [0, L)^3, particle indices are the caller's original indices, energies
+ * are E = 1/2 sum' q_i q_j / r over periodic images (no 4 pi).
+ *
+ * Every call returns an int status (HPDMK_OK = 0) where the reference threw.
+ */
+#ifndef HPDMK_H
+#define HPDMK_H
+
+#include <stddef.h>
+
+#if defined(HPDMK_WITH_MPI)
+#include <mpi.h>
+#else
+/* The library runs on one rank; without MPI the communicator is an opaque int. */
+typedef int MPI_Comm;
+#ifndef MPI_COMM_WORLD
+#define MPI_COMM_WORLD 0
+#endif
+#endif
+
+#ifdef __cplusplus
+typedef enum : int {
+  DIRECT = 1,
+  PROXY = 2,
+} hpdmk_init;
+
+typedef struct HPDMKParams {
+  int n_per_leaf = 200;       /* maximum number of particles per leaf */
+  int digits = 3;             /* 3, 6, 9 or 12 digits of accuracy */
+  double L;                   /* side of the periodic cube */
+  double prolate_order = 16;  /* kept for layout compatibility; unused */
+  hpdmk_init init = PROXY;    /* DIRECT or PROXY (PROXY is limited to 3 digits, as in the reference) */
+} HPDMKParams;
+#else
+typedef enum {
+  DIRECT = 1,
+  PROXY = 2,
+} hpdmk_init;
+
+typedef struct HPDMKParams {
+  int n_per_leaf;
+  int digits;
+  double L;
+  double prolate_order;
+  hpdmk_init init;
+} HPDMKParams;
+#endif
+
+typedef void *hpdmk_tree;
+
+/* status codes */
+#define HPDMK_OK 0
+#define HPDMK_ERR_BAD_PARAMS 1     /* digits not in {3,6,9,12}, L <= 0, n_per_leaf < 1, PROXY with digits > 3 */
+#define HPDMK_ERR_BAD_INPUT 2      /* n < 1, null pointer, position outside [0,L), non-finite value, index out of range */
+#define HPDMK_ERR_CUDA 4           /* CUDA runtime failure (message via hpdmk_last_error_message) */
+#define HPDMK_ERR_OUT_OF_MEMORY 5  /* device allocation failed */
+#define HPDMK_ERR_DEVICE 6         /* device-side error word set (overflow pool exhausted) */
+#define HPDMK_ERR_INTERNAL 7
+
+/* precision modes of hpdmk_tree_init_ext */
+#define HPDMK_PRECISION_FP64 0
+
+typedef struct HPDMKExtParams {
+  int leaf_slack;     /* free particle slots per leaf kept for moves (default 8) */
+  int pool_capacity;  /* overflow slots for arrivals into full leaves (default 4096) */
+  int precision;      /* HPDMK_PRECISION_FP64 */
+  int device;         /* CUDA device ordinal (default 0) */
+  void *stream;       /* cudaStream_t to run on; NULL: the tree creates its own */
+} HPDMKExtParams;
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Reference: include/hpdmk.h:25, src/hpdmk.cpp:18-20 — builds the tree and
+ * discards it (the reference's only C entry point). */
+void hpdmk_tree_create(MPI_Comm comm, HPDMKParams params, int n_src, const double *r_src, const double *charge);
+
+/* Reference: HPDMKPtTree(comm, params, r_src, charge), include/tree.hpp:74 and
+ * src/tree.cpp:267-444. Copies r_src[3n] and charge[n] to the device.
+ * Returns NULL on failure; hpdmk_last_error() tells why. */
+hpdmk_tree hpdmk_tree_init(MPI_Comm comm, HPDMKParams params, int n_src, const double *r_src, const double *charge);
+
+/* As hpdmk_tree_init, with library extensions; ext may be NULL. */
+hpdmk_tree hpdmk_tree_init_ext(MPI_Comm comm, HPDMKParams params, const HPDMKExtParams *ext, int n_src,
+                               const double *r_src, const double *charge);
+
+/* As hpdmk_tree_init_ext with d_r_src[3n] and d_charge[n] already in device memory
+ * (positions are validated on the device). */
+hpdmk_tree hpdmk_tree_init_device(MPI_Comm comm, HPDMKParams params, const HPDMKExtParams *ext, int n_src,
+                                  const double *d_r_src, const double *d_charge);
+
+void hpdmk_tree_destroy(hpdmk_tree tree);
+
+/* Reference: form_outgoing_pw (include/tree.hpp:102, src/planewave.cpp:86-97). */
+int hpdmk_form_outgoing_pw(hpdmk_tree tree);
+
+/* Reference: form_incoming_pw (include/tree.hpp:103, src/planewave.cpp:99-155). */
+int hpdmk_form_incoming_pw(hpdmk_tree tree);
+
+/* Reference: eval_energy = eval_energy_window + eval_energy_diff + eval_energy_res
+ * (include/tree.hpp:105-108, src/energy.cpp:21-173). Any of the part pointers may be NULL. */
+int hpdmk_eval_energy(hpdmk_tree tree, double *energy, double *window, double *difference, double *residual);
+
+/* Convenience: form_outgoing_pw + form_incoming_pw + eval_energy. */
+int hpdmk_energy(hpdmk_tree tree, double *energy);
+
+/* Reference: eval_shift_energy(i, dx, dy, dz) (include/tree.hpp:122, src/energy_shift.cpp:18-70):
+ * energy change of moving original particle i by (dx,dy,dz), wrapped into the box. */
+int hpdmk_eval_shift_energy(hpdmk_tree tree, long i, double dx, double dy, double dz, double *dE);
+
+/* Reference: update_shift(i, dx, dy, dz) (include/tree.hpp:132, src/tree.cpp:447-597):
+ * commit the move; meant to follow hpdmk_eval_shift_energy with the same arguments
+ * (the move is re-evaluated when the arguments differ). */
+int hpdmk_update_shift(hpdmk_tree tree, long i, double dx, double dy, double dz);
+
+/* Batched extension: dE[c] for m candidate moves (i[c], d[3c..3c+2]) against the
+ * current state; no state change. Host arrays. */
+int hpdmk_eval_shift_energy_batch(hpdmk_tree tree, int m, const long *i, const double *d, double *dE);
+
+/* Batched extension: n sequential Metropolis moves at inverse temperature beta.
+ * Move c proposes (i[c], d[3c..]) and is accepted when u[c] < exp(-beta dE);
+ * accepted moves are committed before the next one. Outputs dE[c], accepted[c]
+ * (either may be NULL). Host arrays. */
+int hpdmk_mc_run(hpdmk_tree tree, int n, const long *i, const double *d, const double *u, double beta, double *dE,
+                 int *accepted);
+
+/* As hpdmk_mc_run with device-resident int32 indices and device outputs, enqueued on
+ * the tree's stream without a host synchronisation (stream may be NULL for the default). */
+int hpdmk_mc_run_device(hpdmk_tree tree, int n, const int *d_i, const double *d_d, const double *d_u, double beta,
+                        double *d_dE, int *d_accepted);
+
+/* Current positions in the caller's original order, r[3n]. */
+int hpdmk_get_positions(hpdmk_tree tree, double *r);
+
+/* Tree shape: info[0] number of levels, info[1] nodes, info[2] particles,
+ * info[3] window modes, info[4] difference modes per box. */
+int hpdmk_tree_info(hpdmk_tree tree, long *info);
+
+/* Wait for all queued work of the tree. */
+int hpdmk_synchronize(hpdmk_tree tree);
+
+/* The CUDA stream (cudaStream_t) all work of the tree is enqueued on. */
+int hpdmk_get_stream(hpdmk_tree tree, void **stream);
+
+/* Kernel timing: with enable != 0, CUDA events bracket every shift, update and
+ * outgoing-expansion launch on the tree's stream. hpdmk_get_timing synchronises and
+ * returns, per kernel class c (0 shift, 1 update pair, 2 commit, 3 outgoing NUDFT),
+ * out[2c] = total milliseconds and out[2c+1] = number of launches since the last reset. */
+int hpdmk_set_timing(hpdmk_tree tree, int enable);
+int hpdmk_get_timing(hpdmk_tree tree, double *out, int reset);
+
+/* Work counters of the last MC batch: out[0] accepted moves, out[1] bytes of
+ * expansion data read+written by their updates (algorithmic: 32 B per complex RMW). */
+int hpdmk_get_update_bytes(hpdmk_tree tree, double *out);
+
+/* Last status of the calling thread and its message. */
+int hpdmk_last_error(void);
+const char *hpdmk_last_error_message(void);
+
+/* Introspection used by the parity tests (not part of the reference interface). */
+int hpdmk_debug_nodes(hpdmk_tree tree, int *level, unsigned long long *prefix, int *is_leaf, long *count);
+int hpdmk_debug_neighbors(hpdmk_tree tree, int *colleague27, int *coarse8);
+int hpdmk_debug_sorted_order(hpdmk_tree tree, long *orig_of_sorted);
+int hpdmk_debug_pw(hpdmk_tree tree, long node, int which, double *out);
+int hpdmk_debug_kernels(hpdmk_tree tree, int level, double *out);
+int hpdmk_debug_shift_parts(hpdmk_tree tree, long i, double dx, double dy, double dz, double *parts);
+/* Host-only PSWF set-up for a digits setting: out[0] c, out[1] lambda, out[2] C0 / psi0(0),
+ * out[3] diff0, out[4] n_window, out[5] n_diff; psi[k] = psi0(x[k]) / psi0(0) for k < nx. */
+int hpdmk_debug_prolate(int digits, double *out, int nx, const double *x, double *psi);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPDMK_H */

@@ -1,0 +1,424 @@
+// The C-ABI boundary: plain pointers and sizes in, status codes out. Every
+// exception of the C++ layer is caught here (the reference throws
+// std::runtime_error / std::invalid_argument, src/tree.cpp:21-27,
+// include/utils.hpp:47, src/upward_pass.cpp:13).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/hpdmk.h"
+#include "tree.hpp"
+
+namespace {
+
+thread_local int g_last_error = HPDMK_OK;
+thread_local std::string g_last_message;
+
+struct Handle {
+  std::unique_ptr<pdmk::DmkTree> tree;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  long n = 0;
+  double L = 0;
+  int device = 0;
+  // staging buffers for the host-array batched calls
+  int* d_i = nullptr;
+  double* d_d = nullptr;
+  double* d_u = nullptr;
+  double* d_dE = nullptr;
+  int* d_acc = nullptr;
+  int cap = 0;
+  ~Handle() {
+    tree.reset();
+    if (d_i) cudaFree(d_i);
+    if (d_d) cudaFree(d_d);
+    if (d_u) cudaFree(d_u);
+    if (d_dE) cudaFree(d_dE);
+    if (d_acc) cudaFree(d_acc);
+    if (stream && own_stream) cudaStreamDestroy(stream);
+  }
+  void ensure(int m) {
+    if (m <= cap) return;
+    if (d_i) cudaFree(d_i);
+    if (d_d) cudaFree(d_d);
+    if (d_u) cudaFree(d_u);
+    if (d_dE) cudaFree(d_dE);
+    if (d_acc) cudaFree(d_acc);
+    d_i = nullptr;
+    d_d = d_u = d_dE = nullptr;
+    d_acc = nullptr;
+    cap = 0;
+    PDMK_CUDA(cudaMalloc(&d_i, sizeof(int) * m));
+    PDMK_CUDA(cudaMalloc(&d_d, sizeof(double) * 3 * m));
+    PDMK_CUDA(cudaMalloc(&d_u, sizeof(double) * m));
+    PDMK_CUDA(cudaMalloc(&d_dE, sizeof(double) * m));
+    PDMK_CUDA(cudaMalloc(&d_acc, sizeof(int) * m));
+    cap = m;
+  }
+};
+
+int fail(int code, const std::string& msg) {
+  g_last_error = code;
+  g_last_message = msg;
+  return code;
+}
+
+int ok() {
+  g_last_error = HPDMK_OK;
+  g_last_message.clear();
+  return HPDMK_OK;
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc& e) {
+    return fail(HPDMK_ERR_OUT_OF_MEMORY, e.what());
+  } catch (const pdmk::CudaError& e) {
+    std::string m = e.what();
+    if (m.find("out of memory") != std::string::npos) return fail(HPDMK_ERR_OUT_OF_MEMORY, m);
+    return fail(HPDMK_ERR_CUDA, m);
+  } catch (const std::invalid_argument& e) {
+    return fail(HPDMK_ERR_BAD_PARAMS, e.what());
+  } catch (const std::exception& e) {
+    return fail(HPDMK_ERR_INTERNAL, e.what());
+  }
+}
+
+Handle* H(hpdmk_tree t) { return static_cast<Handle*>(t); }
+
+int check_params(const HPDMKParams& p) {
+  if (!(p.L > 0) || !std::isfinite(p.L)) return fail(HPDMK_ERR_BAD_PARAMS, "L must be positive and finite");
+  if (p.n_per_leaf < 1) return fail(HPDMK_ERR_BAD_PARAMS, "n_per_leaf must be >= 1");
+  if (p.digits != 3 && p.digits != 6 && p.digits != 9 && p.digits != 12)
+    return fail(HPDMK_ERR_BAD_PARAMS, "double only supports 3, 6, 9 and 12 digits accuracy");
+  if (p.init != DIRECT && p.init != PROXY) return fail(HPDMK_ERR_BAD_PARAMS, "init must be DIRECT or PROXY");
+  if (p.init == PROXY && p.digits > 3)
+    return fail(HPDMK_ERR_BAD_PARAMS, "PROXY initialisation supports 3 digits only; use DIRECT");
+  return HPDMK_OK;
+}
+
+int check_inputs(double L, int n, const double* r, const double* q) {
+  if (n < 1 || !r || !q) return fail(HPDMK_ERR_BAD_INPUT, "need n >= 1 particles with positions and charges");
+  for (long k = 0; k < 3L * n; ++k)
+    if (!(r[k] >= 0.0 && r[k] < L)) return fail(HPDMK_ERR_BAD_INPUT, "positions must lie in [0, L)");
+  for (long k = 0; k < n; ++k)
+    if (!std::isfinite(q[k])) return fail(HPDMK_ERR_BAD_INPUT, "charges must be finite");
+  return HPDMK_OK;
+}
+
+int check_move(const Handle* h, long i, double dx, double dy, double dz) {
+  if (i < 0 || i >= h->n) return fail(HPDMK_ERR_BAD_INPUT, "particle index out of range");
+  const double lim = 64.0 * h->L;
+  if (!(std::fabs(dx) < lim && std::fabs(dy) < lim && std::fabs(dz) < lim))
+    return fail(HPDMK_ERR_BAD_INPUT, "displacement must be finite and below 64 L");
+  return HPDMK_OK;
+}
+
+hpdmk_tree init_impl(HPDMKParams params, const HPDMKExtParams* ext, int n, const double* r, const double* q,
+                     bool on_device = false) {
+  if (check_params(params) != HPDMK_OK) return nullptr;
+  if (on_device) {
+    if (n < 1 || !r || !q) {
+      fail(HPDMK_ERR_BAD_INPUT, "need n >= 1 particles with positions and charges");
+      return nullptr;
+    }
+  } else if (check_inputs(params.L, n, r, q) != HPDMK_OK) {
+    return nullptr;
+  }
+  Handle* h = nullptr;
+  int st = guarded([&]() {
+    auto hh = std::make_unique<Handle>();
+    pdmk::TreeOptions opt;
+    opt.leaf_slack = ext ? ext->leaf_slack : 8;
+    opt.pool_capacity = ext && ext->pool_capacity > 0 ? ext->pool_capacity : 4096;
+    if (opt.leaf_slack < 0) return fail(HPDMK_ERR_BAD_PARAMS, "leaf_slack must be >= 0");
+    if (ext && ext->precision != HPDMK_PRECISION_FP64) return fail(HPDMK_ERR_BAD_PARAMS, "unknown precision mode");
+    hh->device = ext ? ext->device : 0;
+    PDMK_CUDA(cudaSetDevice(hh->device));
+    if (ext && ext->stream) {
+      hh->stream = static_cast<cudaStream_t>(ext->stream);
+      hh->own_stream = false;
+    } else {
+      PDMK_CUDA(cudaStreamCreateWithFlags(&hh->stream, cudaStreamNonBlocking));
+    }
+    hh->n = n;
+    hh->L = params.L;
+    if (on_device && !pdmk::device_positions_valid(r, q, n, params.L, hh->stream))
+      return fail(HPDMK_ERR_BAD_INPUT, "positions must lie in [0, L) and charges be finite");
+    hh->tree = std::make_unique<pdmk::DmkTree>(params.L, params.n_per_leaf, params.digits, n, r, q, on_device, opt,
+                                               hh->stream);
+    h = hh.release();
+    return ok();
+  });
+  return st == HPDMK_OK ? h : nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+void hpdmk_tree_create(MPI_Comm, HPDMKParams params, int n_src, const double* r_src, const double* charge) {
+  hpdmk_tree t = init_impl(params, nullptr, n_src, r_src, charge);
+  if (t) delete H(t);
+}
+
+hpdmk_tree hpdmk_tree_init(MPI_Comm, HPDMKParams params, int n_src, const double* r_src, const double* charge) {
+  return init_impl(params, nullptr, n_src, r_src, charge);
+}
+
+hpdmk_tree hpdmk_tree_init_ext(MPI_Comm, HPDMKParams params, const HPDMKExtParams* ext, int n_src,
+                               const double* r_src, const double* charge) {
+  return init_impl(params, ext, n_src, r_src, charge);
+}
+
+hpdmk_tree hpdmk_tree_init_device(MPI_Comm, HPDMKParams params, const HPDMKExtParams* ext, int n_src,
+                                  const double* d_r_src, const double* d_charge) {
+  return init_impl(params, ext, n_src, d_r_src, d_charge, true);
+}
+
+void hpdmk_tree_destroy(hpdmk_tree tree) {
+  if (tree) delete H(tree);
+}
+
+int hpdmk_form_outgoing_pw(hpdmk_tree t) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  return guarded([&]() {
+    H(t)->tree->form_outgoing_pw();
+    return ok();
+  });
+}
+
+int hpdmk_form_incoming_pw(hpdmk_tree t) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  return guarded([&]() {
+    H(t)->tree->form_incoming_pw();
+    return ok();
+  });
+}
+
+int hpdmk_eval_energy(hpdmk_tree t, double* energy, double* window, double* difference, double* residual) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  return guarded([&]() {
+    pdmk::EnergyParts p = H(t)->tree->eval_energy();
+    if (energy) *energy = p.total();
+    if (window) *window = p.window;
+    if (difference) *difference = p.diff;
+    if (residual) *residual = p.res;
+    return ok();
+  });
+}
+
+int hpdmk_energy(hpdmk_tree t, double* energy) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  return guarded([&]() {
+    auto* tr = H(t)->tree.get();
+    tr->form_outgoing_pw();
+    tr->form_incoming_pw();
+    pdmk::EnergyParts p = tr->eval_energy();
+    if (energy) *energy = p.total();
+    return ok();
+  });
+}
+
+int hpdmk_eval_shift_energy(hpdmk_tree t, long i, double dx, double dy, double dz, double* dE) {
+  if (!t || !dE) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  if (check_move(H(t), i, dx, dy, dz) != HPDMK_OK) return g_last_error;
+  return guarded([&]() {
+    *dE = H(t)->tree->eval_shift_energy(i, dx, dy, dz, nullptr);
+    return ok();
+  });
+}
+
+int hpdmk_debug_shift_parts(hpdmk_tree t, long i, double dx, double dy, double dz, double* parts) {
+  if (!t || !parts) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  if (check_move(H(t), i, dx, dy, dz) != HPDMK_OK) return g_last_error;
+  return guarded([&]() {
+    H(t)->tree->eval_shift_energy(i, dx, dy, dz, parts);
+    return ok();
+  });
+}
+
+int hpdmk_update_shift(hpdmk_tree t, long i, double dx, double dy, double dz) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  if (check_move(H(t), i, dx, dy, dz) != HPDMK_OK) return g_last_error;
+  return guarded([&]() {
+    H(t)->tree->update_shift(i, dx, dy, dz);
+    if (H(t)->tree->check_device_error()) return fail(HPDMK_ERR_DEVICE, "overflow pool exhausted");
+    return ok();
+  });
+}
+
+int hpdmk_eval_shift_energy_batch(hpdmk_tree t, int m, const long* i, const double* d, double* dE) {
+  if (!t || m < 0 || (m > 0 && (!i || !d || !dE))) return fail(HPDMK_ERR_BAD_INPUT, "bad batch arguments");
+  Handle* h = H(t);
+  for (int c = 0; c < m; ++c)
+    if (check_move(h, i[c], d[3 * c], d[3 * c + 1], d[3 * c + 2]) != HPDMK_OK) return g_last_error;
+  if (m == 0) return ok();
+  return guarded([&]() {
+    h->ensure(m);
+    std::vector<int> ii(i, i + m);
+    PDMK_CUDA(cudaMemcpyAsync(h->d_i, ii.data(), sizeof(int) * m, cudaMemcpyHostToDevice, h->stream));
+    PDMK_CUDA(cudaMemcpyAsync(h->d_d, d, sizeof(double) * 3 * m, cudaMemcpyHostToDevice, h->stream));
+    h->tree->shift_batch_device(m, h->d_i, h->d_d, h->d_dE);
+    PDMK_CUDA(cudaMemcpyAsync(dE, h->d_dE, sizeof(double) * m, cudaMemcpyDeviceToHost, h->stream));
+    PDMK_CUDA(cudaStreamSynchronize(h->stream));
+    return ok();
+  });
+}
+
+int hpdmk_mc_run(hpdmk_tree t, int n, const long* i, const double* d, const double* u, double beta, double* dE,
+                 int* accepted) {
+  if (!t || n < 0 || (n > 0 && (!i || !d || !u))) return fail(HPDMK_ERR_BAD_INPUT, "bad move arguments");
+  Handle* h = H(t);
+  for (int c = 0; c < n; ++c)
+    if (check_move(h, i[c], d[3 * c], d[3 * c + 1], d[3 * c + 2]) != HPDMK_OK) return g_last_error;
+  if (n == 0) return ok();
+  return guarded([&]() {
+    h->ensure(n);
+    std::vector<int> ii(i, i + n);
+    PDMK_CUDA(cudaMemcpyAsync(h->d_i, ii.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    PDMK_CUDA(cudaMemcpyAsync(h->d_d, d, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
+    PDMK_CUDA(cudaMemcpyAsync(h->d_u, u, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    h->tree->reset_work();
+    h->tree->mc_run_device(n, h->d_i, h->d_d, h->d_u, beta, h->d_dE, h->d_acc);
+    if (dE) PDMK_CUDA(cudaMemcpyAsync(dE, h->d_dE, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    if (accepted) PDMK_CUDA(cudaMemcpyAsync(accepted, h->d_acc, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+    PDMK_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->tree->check_device_error()) return fail(HPDMK_ERR_DEVICE, "overflow pool exhausted");
+    return ok();
+  });
+}
+
+int hpdmk_mc_run_device(hpdmk_tree t, int n, const int* d_i, const double* d_d, const double* d_u, double beta,
+                        double* d_dE, int* d_accepted) {
+  if (!t || n < 0 || (n > 0 && (!d_i || !d_d || !d_u))) return fail(HPDMK_ERR_BAD_INPUT, "bad move arguments");
+  return guarded([&]() {
+    H(t)->tree->reset_work();
+    H(t)->tree->mc_run_device(n, d_i, d_d, d_u, beta, d_dE, d_accepted);
+    return ok();
+  });
+}
+
+int hpdmk_get_positions(hpdmk_tree t, double* r) {
+  if (!t || !r) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  return guarded([&]() {
+    H(t)->tree->export_positions(r);
+    return ok();
+  });
+}
+
+int hpdmk_tree_info(hpdmk_tree t, long* info) {
+  if (!t || !info) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  const auto& D = H(t)->tree->dev();
+  info[0] = D.max_depth;
+  info[1] = D.n_nodes;
+  info[2] = D.N;
+  info[3] = D.Hw;
+  info[4] = D.H;
+  return ok();
+}
+
+int hpdmk_synchronize(hpdmk_tree t) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  return guarded([&]() {
+    H(t)->tree->synchronize();
+    return ok();
+  });
+}
+
+int hpdmk_get_stream(hpdmk_tree t, void** stream) {
+  if (!t || !stream) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  *stream = static_cast<void*>(H(t)->stream);
+  return ok();
+}
+
+int hpdmk_set_timing(hpdmk_tree t, int enable) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  H(t)->tree->set_timing(enable != 0);
+  return ok();
+}
+
+int hpdmk_get_timing(hpdmk_tree t, double* out, int reset) {
+  if (!t || !out) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  return guarded([&]() {
+    H(t)->tree->get_timing(out, reset != 0);
+    return ok();
+  });
+}
+
+int hpdmk_get_update_bytes(hpdmk_tree t, double* out) {
+  if (!t || !out) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  return guarded([&]() {
+    H(t)->tree->get_work(out);
+    return ok();
+  });
+}
+
+int hpdmk_last_error(void) { return g_last_error; }
+const char* hpdmk_last_error_message(void) { return g_last_message.c_str(); }
+
+int hpdmk_debug_nodes(hpdmk_tree t, int* level, unsigned long long* prefix, int* is_leaf, long* count) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  return guarded([&]() {
+    H(t)->tree->export_nodes(level, reinterpret_cast<uint64_t*>(prefix), is_leaf, count);
+    return ok();
+  });
+}
+
+int hpdmk_debug_neighbors(hpdmk_tree t, int* col27, int* coarse8) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  return guarded([&]() {
+    H(t)->tree->export_neighbors(col27, coarse8);
+    return ok();
+  });
+}
+
+int hpdmk_debug_sorted_order(hpdmk_tree t, long* o) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  return guarded([&]() {
+    H(t)->tree->export_sorted_order(o);
+    return ok();
+  });
+}
+
+int hpdmk_debug_pw(hpdmk_tree t, long node, int which, double* out) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  return guarded([&]() {
+    H(t)->tree->export_pw(node, which, out);
+    return ok();
+  });
+}
+
+int hpdmk_debug_kernels(hpdmk_tree t, int level, double* out) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  return guarded([&]() {
+    if (level == 0) H(t)->tree->export_W(out);
+    else H(t)->tree->export_D(level, out);
+    return ok();
+  });
+}
+
+int hpdmk_debug_prolate(int digits, double* out, int nx, const double* x, double* psi) {
+  if (!out || (nx > 0 && (!x || !psi))) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  return guarded([&]() {
+    pdmk::ProlateSetup s = pdmk::make_prolate_setup(digits);
+    out[0] = s.c;
+    out[1] = s.lambda;
+    out[2] = s.C0 / s.psi0_0;
+    out[3] = s.diff0;
+    out[4] = s.n_window;
+    out[5] = s.n_diff;
+    for (int k = 0; k < nx; ++k) psi[k] = s.psi0(x[k]) / s.psi0_0;
+    return ok();
+  });
+}
+
+}  // extern "C"

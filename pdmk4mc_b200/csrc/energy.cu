@@ -1,0 +1,707 @@
+// Full-energy kernels (FP64): the plane-wave upward pass, incoming
+// expansions, window / difference / residual energies.
+//
+// Reference counterparts: outgoing_pw_root / outgoing_pw_direct and
+// nudft3d1_halfplane (src/planewave.cpp:24-84, include/nudft.hpp:66-123),
+// form_incoming_pw (src/planewave.cpp:99-155), eval_energy_window /
+// eval_energy_diff / eval_energy_res (src/energy.cpp:21-173).
+//
+// The outgoing expansion of a box, rho_B(k) = sum_j q_j exp(-i k.x_j) over
+// the half grid kz <= 0, is evaluated as the complex contraction
+//   out[(kz,ky), kx] = sum_j (q_j ez_j[kz] ey_j[ky]) ex_j[kx]
+// with box-centred coordinates: exp(-i k.x) = exp(-i k.c_B) exp(-i k.(x-c_B)),
+// where k.c_B is an exact multiple of pi/3 (k = m dk_l, dk_l bs_l = 2 pi / 3),
+// so the decentring factor is an exact sixth root of unity per axis.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "tree.hpp"
+
+namespace pdmk {
+namespace {
+
+constexpr int TPB = 256;
+inline unsigned grid_for(long n, int tpb = TPB) { return unsigned(std::max<long>(1, (n + tpb - 1) / tpb)); }
+
+__device__ inline double block_sum(double v, double* sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) sm[warp] = v;
+  __syncthreads();
+  double s = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < nw; ++w) s += sm[w];
+  return s;  // valid in thread 0
+}
+
+// ---------------------------------------------------------------------------
+// NUDFT work item: one row tile of one box over one slot range
+struct NudftWork {
+  double cx, cy, cz;  // box centre
+  double dk;
+  int X, Y, Z;        // integer box coordinates at its level
+  int M;              // decentring multiplier: 1 for levels >= 2, 3 for the root
+  int s_begin, s_end;
+  int row_tile;
+  int pad_;
+  double2* out;       // H complex outputs of this box (or of this split-K chunk)
+};
+
+template <int NK>
+struct NudftShape {
+  static constexpr int D = 2 * NK + 1;
+  static constexpr int CG = D > 40 ? 2 : 1;           // column groups per row
+  static constexpr int TC = (D + CG - 1) / CG;        // columns per thread
+  static constexpr int DP = TC * CG;                  // padded row stride in smem
+  static constexpr int ROWS = (NK + 1) * D;
+  static constexpr int WORK = ROWS * CG;              // thread tasks per box
+  static constexpr int TMAX = D > 30 ? 288 : 352;
+  static constexpr int TILES = (WORK + TMAX - 1) / TMAX;
+  static constexpr int THREADS = ((WORK + TILES - 1) / TILES + 31) / 32 * 32;
+  static constexpr int KC = 16;                       // particles per shared-memory chunk
+  static constexpr int SMEM = KC * (2 * DP + NK + 1) * int(sizeof(double2));
+};
+
+// per-axis factors exp(-i m dk (x - c)) * w6^{-M (2X+1) m}, m = m0 .. m0+cnt-1
+__device__ inline void axis_factors(double xr, double dk, int M, int X, int m0, int cnt, double scale, double2* dst) {
+  double th = dk * xr;
+  double s, c;
+  sincos(-double(m0) * th, &s, &c);
+  double2 v = make_double2(c * scale, s * scale);
+  sincos(-th, &s, &c);
+  const double2 step = make_double2(c, s);
+  const int dec = M * (2 * X + 1);
+  for (int t = 0; t < cnt; ++t) {
+    int m = m0 + t;
+    dst[t] = cmul(v, root6(-dec * m));
+    v = cmul(v, step);
+  }
+}
+
+template <int NK>
+__global__ void __launch_bounds__(NudftShape<NK>::THREADS)
+    k_nudft(const NudftWork* __restrict__ work, const double* __restrict__ sx, const double* __restrict__ sy,
+            const double* __restrict__ sz, const double* __restrict__ sq) {
+  using S = NudftShape<NK>;
+  extern __shared__ double2 smem[];
+  double2* ex = smem;                    // [KC][DP]
+  double2* ey = ex + S::KC * S::DP;      // [KC][DP]
+  double2* ez = ey + S::KC * S::DP;      // [KC][NK+1], charge folded in
+  const NudftWork w = work[blockIdx.x];
+  const int g = w.row_tile * S::THREADS + threadIdx.x;
+  const bool active = g < S::WORK;
+  const int row = active ? g / S::CG : 0;
+  const int cg = active ? g % S::CG : 0;
+  const int kz = row / S::D, ky = row % S::D;
+  const int c0 = cg * S::TC;
+  double2 acc[S::TC];
+#pragma unroll
+  for (int c = 0; c < S::TC; ++c) acc[c] = make_double2(0.0, 0.0);
+  for (int base = w.s_begin; base < w.s_end; base += S::KC) {
+    const int nk = min(S::KC, w.s_end - base);
+    __syncthreads();
+    // factor tables: (particle, axis, half) tasks
+    for (int t = threadIdx.x; t < S::KC * 6; t += blockDim.x) {
+      int j = t / 6, a = (t / 2) % 3, half = t & 1;
+      if (j >= nk) {
+        // zero rows so the inner loop needs no bound
+        double2* dst = a == 0 ? ex + j * S::DP : (a == 1 ? ey + j * S::DP : ez + j * (NK + 1));
+        int len = a == 2 ? NK + 1 : S::DP;
+        for (int u = half; u < len; u += 2) dst[u] = make_double2(0.0, 0.0);
+        continue;
+      }
+      int s = base + j;
+      if (a == 0) {
+        int h = (S::D + 1) / 2;
+        int m0 = half ? -NK + h : -NK, cnt = half ? S::D - h : h;
+        axis_factors(sx[s] - w.cx, w.dk, w.M, w.X, m0, cnt, 1.0, ex + j * S::DP + (m0 + NK));
+        if (half)
+          for (int u = S::D; u < S::DP; ++u) ex[j * S::DP + u] = make_double2(0.0, 0.0);
+      } else if (a == 1) {
+        int h = (S::D + 1) / 2;
+        int m0 = half ? -NK + h : -NK, cnt = half ? S::D - h : h;
+        axis_factors(sy[s] - w.cy, w.dk, w.M, w.Y, m0, cnt, 1.0, ey + j * S::DP + (m0 + NK));
+      } else {
+        int h = (NK + 2) / 2;
+        int m0 = half ? -NK + h : -NK, cnt = half ? NK + 1 - h : h;
+        axis_factors(sz[s] - w.cz, w.dk, w.M, w.Z, m0, cnt, sq[s], ez + j * (NK + 1) + (m0 + NK));
+      }
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll 2
+      for (int j = 0; j < nk; ++j) {
+        const double2 a = cmul(ez[j * (NK + 1) + kz], ey[j * S::DP + ky]);
+        const double2* xr = ex + j * S::DP + c0;
+#pragma unroll
+        for (int c = 0; c < S::TC; ++c) {
+          const double2 b = xr[c];
+          acc[c].x = fma(a.x, b.x, acc[c].x);
+          acc[c].x = fma(-a.y, b.y, acc[c].x);
+          acc[c].y = fma(a.x, b.y, acc[c].y);
+          acc[c].y = fma(a.y, b.x, acc[c].y);
+        }
+      }
+    }
+  }
+  if (active) {
+    double2* o = w.out + size_t(row) * S::D + c0;
+#pragma unroll
+    for (int c = 0; c < S::TC; ++c)
+      if (c0 + c < S::D) o[c] = acc[c];
+  }
+}
+
+template <int NK>
+void launch_nudft(const NudftWork* d_work, int nwork, const DevTree& T, cudaStream_t st) {
+  using S = NudftShape<NK>;
+  if (nwork == 0) return;
+  static bool attr = false;
+  if (!attr) {
+    PDMK_CUDA(cudaFuncSetAttribute(k_nudft<NK>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
+    attr = true;
+  }
+  k_nudft<NK><<<unsigned(nwork), S::THREADS, S::SMEM, st>>>(d_work, T.sx, T.sy, T.sz, T.sq);
+  PDMK_LAUNCH_CHECK();
+}
+
+void dispatch_nudft(int nk, const NudftWork* d_work, int nwork, const DevTree& T, cudaStream_t st) {
+  switch (nk) {
+    case 4: launch_nudft<4>(d_work, nwork, T, st); break;
+    case 6: launch_nudft<6>(d_work, nwork, T, st); break;
+    case 8: launch_nudft<8>(d_work, nwork, T, st); break;
+    case 12: launch_nudft<12>(d_work, nwork, T, st); break;
+    case 13: launch_nudft<13>(d_work, nwork, T, st); break;
+    case 17: launch_nudft<17>(d_work, nwork, T, st); break;
+    case 19: launch_nudft<19>(d_work, nwork, T, st); break;
+    case 26: launch_nudft<26>(d_work, nwork, T, st); break;
+    default: throw std::invalid_argument("unsupported mode count");
+  }
+}
+
+int nudft_tiles(int nk) {
+  switch (nk) {
+    case 4: return NudftShape<4>::TILES;
+    case 6: return NudftShape<6>::TILES;
+    case 8: return NudftShape<8>::TILES;
+    case 12: return NudftShape<12>::TILES;
+    case 13: return NudftShape<13>::TILES;
+    case 17: return NudftShape<17>::TILES;
+    case 19: return NudftShape<19>::TILES;
+    case 26: return NudftShape<26>::TILES;
+    default: throw std::invalid_argument("unsupported mode count");
+  }
+}
+
+// sum split-K chunk partials of box b into its output, in chunk order
+__global__ void k_reduce_chunks(const double2* part, const int* chunk_first, const int* chunk_n, double2* const* outs,
+                                int H) {
+  int b = blockIdx.y;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= H) return;
+  const double2* p = part + size_t(chunk_first[b]) * H + k;
+  double2 s = make_double2(0, 0);
+  for (int c = 0; c < chunk_n[b]; ++c) s = cadd(s, p[size_t(c) * H]);
+  outs[b][k] = s;
+}
+
+// ---------------------------------------------------------------------------
+__device__ inline int wrap_flag(int X, int d, int l) {
+  int v = X + d;
+  return v < 0 ? -1 : (v >= (1 << l) ? 1 : 0);
+}
+
+// inc_B = conj(out_B) + sum_C conj(out_C * exp(-i k.p L)), with the energy
+// sum Re(out_B inc_B) D_2 per (box, k tile); ktile-major grid order keeps the
+// colleagues' tiles resident in L2.
+__global__ void k_incoming(DevTree T, const int* __restrict__ boxes, int nboxes, int write_inc, double* part) {
+  __shared__ double sm[32];
+  const int tile = blockIdx.x / nboxes, b = blockIdx.x % nboxes;
+  const int node = boxes[b];
+  const int l = T.node_level[node];
+  const uint64_t p = T.node_prefix[node];
+  const int X = compact3(p), Y = compact3(p >> 1), Z = compact3(p >> 2);
+  const int n = T.n_diff, d = T.dd;
+  const int k = tile * blockDim.x + threadIdx.x;
+  const int base = T.level_start[T.pw_lo];
+  double e = 0;
+  if (k < T.H) {
+    const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
+    const int two_l_mod3 = (l & 1) ? 2 : 1;
+    const double2* outB = T.out + size_t(node - base) * T.H;
+    double2 acc = T.node_count[node] > 0 ? cconj(outB[k]) : make_double2(0, 0);
+    const int* col = T.col27 + size_t(node) * 27;
+    for (int dir = 0; dir < 27; ++dir) {
+      int j = col[dir];
+      if (j < 0 || T.node_count[j] == 0) continue;
+      int dx = dir % 3 - 1, dy = (dir / 3) % 3 - 1, dz = dir / 9 - 1;
+      // image offset of the source colleague as seen from B (periodic_shift(c_C, c_B))
+      int px = wrap_flag(X, dx, l), py = wrap_flag(Y, dy, l), pz = wrap_flag(Z, dz, l);
+      double2 v = T.out[size_t(j - base) * T.H + k];
+      if (px | py | pz) {
+        int sgn = ((ix - n) * px + (iy - n) * py + (iz - n) * pz) * two_l_mod3;
+        // exp(-i 2 pi sgn / 3) = w6^{-2 sgn}
+        v = cmul(v, root6(-2 * (sgn % 3)));
+      }
+      acc = cadd(acc, cconj(v));
+    }
+    if (write_inc) T.inc[size_t(node - base) * T.H + k] = acc;
+    const double2 o = outB[k];
+    e = (o.x * acc.x - o.y * acc.y) * T.D2[k];
+  }
+  double s = block_sum(e, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// Re sum out_B inc_B D_2 per (box, k tile) on the stored incoming expansions
+__global__ void k_tridot(DevTree T, const int* __restrict__ boxes, int nboxes, double* part) {
+  __shared__ double sm[32];
+  const int tile = blockIdx.x / nboxes, b = blockIdx.x % nboxes;
+  const int node = boxes[b];
+  const int k = tile * blockDim.x + threadIdx.x;
+  const int base = T.level_start[T.pw_lo];
+  double e = 0;
+  if (k < T.H) {
+    double2 o = T.out[size_t(node - base) * T.H + k];
+    double2 c = T.inc[size_t(node - base) * T.H + k];
+    e = (o.x * c.x - o.y * c.y) * T.D2[k];
+  }
+  double s = block_sum(e, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// sum of q^2 over each box's slots
+__global__ void k_box_q2(DevTree T, const int* __restrict__ boxes, double* q2) {
+  __shared__ double sm[32];
+  int node = boxes[blockIdx.x];
+  double v = 0;
+  for (int s = T.node_begin[node] + threadIdx.x; s < T.node_end[node]; s += blockDim.x) v += T.sq[s] * T.sq[s];
+  double tot = block_sum(v, sm);
+  if (threadIdx.x == 0) q2[blockIdx.x] = tot;
+}
+
+// E_diff = sum_box [C_l dscale_l sum_tiles part - Q_B S_l]
+__global__ void k_diff_finish(DevTree T, const int* __restrict__ boxes, int nboxes, int ktiles, const double* part,
+                              const double* q2, const double* Cl, const double* Sl, double* out) {
+  __shared__ double sm[32];
+  double e = 0;
+  for (int b = threadIdx.x; b < nboxes; b += blockDim.x) {
+    int node = boxes[b];
+    int l = T.node_level[node];
+    double t = 0;
+    for (int tile = 0; tile < ktiles; ++tile) t += part[size_t(tile) * nboxes + b];
+    e += Cl[l] * T.dscale[l] * t - q2[b] * Sl[l];
+  }
+  double s = block_sum(e, sm);
+  if (threadIdx.x == 0) *out = s;
+}
+
+__global__ void k_window(DevTree T, double scale, double self, double* out) {
+  __shared__ double sm[32];
+  double e = 0;
+  for (int k = threadIdx.x; k < T.Hw; k += blockDim.x) {
+    double2 o = T.out_root[k];
+    e += (o.x * o.x + o.y * o.y) * T.W[k];
+  }
+  double s = block_sum(e, sm);
+  if (threadIdx.x == 0) *out = s * scale - self;
+}
+
+// residual_kernel (include/kernels.hpp:50-58) with PolyFun::eval (include/pswf.hpp:70-78)
+__device__ inline double res_kernel(const DevTree& T, double r, double b) {
+  if (r == 0) return 0;
+  double xs = (r / b - 0.5) * 2.0;
+  if (fabs(xs) >= 1.0) return 0;
+  double v = 0;
+  for (int i = 0; i < T.n_poly; ++i) v = fma(v, xs, T.poly[i]);
+  return v / r;
+}
+
+__device__ inline int periodic_shift_d(double xi, double xj, double L, double bi, double bj) {
+  if (xi < bi && xj > (L - bj)) return 1;
+  if (xi > (L - bi) && xj < bj) return -1;
+  return 0;
+}
+
+__device__ inline void node_center(const DevTree& T, int node, double* c) {
+  uint64_t p = T.node_prefix[node];
+  int l = T.node_level[node];
+  double scale = ldexp(1.0, -l);
+  c[0] = T.L * (double(compact3(p)) * scale + 0.5 * scale);
+  c[1] = T.L * (double(compact3(p >> 1)) * scale + 0.5 * scale);
+  c[2] = T.L * (double(compact3(p >> 2)) * scale + 0.5 * scale);
+}
+
+constexpr int RES_T = 128;
+constexpr int RES_CHUNK = 128;
+
+// leaf near field: 1/2 sum_{i in B} q_i sum_{j in N(B), j != i} q_j res(r_ij; bs_B)
+__global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __restrict__ leaves, double* part) {
+  __shared__ double tx[RES_CHUNK], ty[RES_CHUNK], tz[RES_CHUNK], tq[RES_CHUNK];
+  __shared__ double ux[RES_CHUNK], uy[RES_CHUNK], uz[RES_CHUNK], uq[RES_CHUNK];
+  __shared__ double sm[32];
+  const int node = leaves[blockIdx.x];
+  const int l = T.node_level[node];
+  const int cnt = T.leaf_count[node];
+  double e = 0;
+  if (l >= 2 && cnt > 0) {
+    const double b = T.boxsize[l];
+    double ci[3];
+    node_center(T, node, ci);
+    const int tb = T.node_begin[node];
+    for (int t0 = 0; t0 < cnt; t0 += RES_CHUNK) {
+      const int nt = min(RES_CHUNK, cnt - t0);
+      __syncthreads();
+      for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        tx[t] = T.sx[tb + t0 + t];
+        ty[t] = T.sy[tb + t0 + t];
+        tz[t] = T.sz[tb + t0 + t];
+        tq[t] = T.sq[tb + t0 + t];
+      }
+      // sources: self, 26 colleagues, up to 8 coarse-grain neighbours
+      for (int src = 0; src < 35; ++src) {
+        int j;
+        if (src == 0) j = node;
+        else if (src <= 27) {
+          if (src - 1 == 13) continue;
+          j = T.col27[size_t(node) * 27 + (src - 1)];
+        } else {
+          j = T.coarse8[size_t(node) * 8 + (src - 28)];
+        }
+        if (j < 0 || T.node_count[j] == 0) continue;
+        double cj[3];
+        node_center(T, j, cj);
+        const double bj = T.boxsize[T.node_level[j]];
+        double off[3];
+        for (int dd = 0; dd < 3; ++dd) off[dd] = -periodic_shift_d(ci[dd], cj[dd], T.L, b, bj) * T.L;
+        const bool is_leaf = T.node_child0[j] < 0;
+        const int sb = T.node_begin[j];
+        const int se = is_leaf ? sb + T.leaf_count[j] : T.node_end[j];
+        for (int s0 = sb; s0 < se; s0 += RES_CHUNK) {
+          const int ns = min(RES_CHUNK, se - s0);
+          __syncthreads();
+          for (int t = threadIdx.x; t < ns; t += blockDim.x) {
+            ux[t] = T.sx[s0 + t] + off[0];
+            uy[t] = T.sy[s0 + t] + off[1];
+            uz[t] = T.sz[s0 + t] + off[2];
+            uq[t] = T.sq[s0 + t];
+          }
+          __syncthreads();
+          for (int pq = threadIdx.x; pq < nt * ns; pq += blockDim.x) {
+            int it = pq / ns, js = pq % ns;
+            if (src == 0 && s0 + js == tb + t0 + it) continue;
+            double dx = tx[it] - ux[js], dy = ty[it] - uy[js], dz = tz[it] - uz[js];
+            double r = sqrt(dx * dx + dy * dy + dz * dz);
+            if (r <= b) e += tq[it] * uq[js] * res_kernel(T, r, b);
+          }
+        }
+      }
+    }
+  }
+  double s = block_sum(0.5 * e, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void k_sum(const double* part, int n, double* out) {
+  __shared__ double sm[32];
+  double e = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) e += part[i];
+  double s = block_sum(e, sm);
+  if (threadIdx.x == 0) *out = s;
+}
+
+__global__ void k_sum_q2(const double* sq, int n, double* out) {
+  __shared__ double sm[32];
+  double e = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) e += sq[i] * sq[i];
+  double s = block_sum(e, sm);
+  if (threadIdx.x == 0) *out = s;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+
+constexpr int KSPLIT = 4096;  // particles per split-K chunk
+
+size_t DmkTree::partials_needed() const {
+  const DevTree& D = dev_;
+  size_t need = 8192;
+  long n_pw = D.pw_hi >= D.pw_lo ? long(D.level_start[D.pw_hi + 1]) - D.level_start[D.pw_lo] : 0;
+  long ktiles = (D.H + TPB - 1) / TPB;
+  need = std::max<size_t>(need, size_t(n_pw) * ktiles + 2 * size_t(n_pw) + 64);
+  need = std::max<size_t>(need, size_t(D.n_nodes) + 64);
+  return need;
+}
+
+void DmkTree::ensure_packed() {
+  int pn = 0;
+  PDMK_CUDA(cudaMemcpyAsync(&pn, dev_.pool_n, 4, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  if (pn > 0) repack(opt_.leaf_slack);
+}
+
+void DmkTree::form_outgoing_pw() {
+  ensure_packed();
+  DevTree& D = dev_;
+  // host view of node slot ranges and coordinates for the work list
+  const int nn = D.n_nodes;
+  std::vector<int> nb(nn), ne(nn), lv(nn);
+  std::vector<uint64_t> pf(nn);
+  PDMK_CUDA(cudaMemcpyAsync(nb.data(), D.node_begin, 4 * nn, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaMemcpyAsync(ne.data(), D.node_end, 4 * nn, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaMemcpyAsync(lv.data(), D.node_level, 4 * nn, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaMemcpyAsync(pf.data(), D.node_prefix, 8 * nn, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  struct Box {
+    int node, sb, se, level;
+    double2* out;
+  };
+  // root split into chunks + boxes of the expansion levels
+  std::vector<Box> boxes;
+  const int base = D.level_start[D.pw_lo];
+  if (D.pw_hi >= D.pw_lo)
+    for (int id = base; id < D.level_start[D.pw_hi + 1]; ++id)
+      boxes.push_back({id, nb[id], ne[id], lv[id], D.out + size_t(id - base) * D.H});
+  // split-K bookkeeping: chunks go to a partial buffer, then reduce
+  struct Chunked {
+    int first, n;
+    double2* out;
+  };
+  std::vector<Chunked> root_split, box_split;
+  std::vector<NudftWork> wroot, wbox;
+  long part_root = 0, part_box = 0;
+  auto make_work = [&](std::vector<NudftWork>& wl, int nk, const Box& bx, double2* out, int sb, int se) {
+    NudftWork w{};
+    int l = bx.level;
+    uint64_t p = pf[bx.node];
+    double scale = std::ldexp(1.0, -l);
+    int X = int(compact3(p)), Y = int(compact3(p >> 1)), Z = int(compact3(p >> 2));
+    w.cx = L_ * (double(X) * scale + 0.5 * scale);
+    w.cy = L_ * (double(Y) * scale + 0.5 * scale);
+    w.cz = L_ * (double(Z) * scale + 0.5 * scale);
+    w.dk = D.delta_k[l];
+    w.X = X;
+    w.Y = Y;
+    w.Z = Z;
+    w.M = l == 0 ? 3 : 1;
+    w.s_begin = sb;
+    w.s_end = se;
+    w.out = out;
+    int tiles = nudft_tiles(nk);
+    for (int t = 0; t < tiles; ++t) {
+      w.row_tile = t;
+      wl.push_back(w);
+    }
+  };
+  // root over all slots
+  {
+    int nch = std::max(1, (D.n_slots + KSPLIT - 1) / KSPLIT);
+    root_split.push_back({0, nch, D.out_root});
+    part_root = long(nch) * D.Hw;
+  }
+  // boxes: largest first (longest-processing-time order), split when large
+  std::vector<int> order(boxes.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = int(i);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return boxes[a].se - boxes[a].sb > boxes[b].se - boxes[b].sb; });
+  long chunk_cursor = 0;
+  for (int oi : order) {
+    const Box& bx = boxes[oi];
+    int cntp = bx.se - bx.sb;
+    if (cntp > KSPLIT) {
+      int nch = (cntp + KSPLIT - 1) / KSPLIT;
+      box_split.push_back({int(chunk_cursor), nch, bx.out});
+      chunk_cursor += nch;
+    }
+  }
+  part_box = chunk_cursor * D.H;
+  double2* part = nullptr;
+  size_t part_bytes = sizeof(double2) * size_t(part_root + part_box + 1);
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part), part_bytes, st_));
+  double2* part_b = part + part_root;
+  {
+    Box r{0, 0, D.n_slots, 0, D.out_root};
+    int nch = root_split[0].n;
+    for (int c = 0; c < nch; ++c) {
+      int sb = c * KSPLIT, se = std::min(D.n_slots, sb + KSPLIT);
+      make_work(wroot, D.n_window, r, part + size_t(c) * D.Hw, sb, se);
+    }
+  }
+  {
+    size_t si = 0;
+    long cur = 0;
+    for (int oi : order) {
+      const Box& bx = boxes[oi];
+      int cntp = bx.se - bx.sb;
+      if (cntp > KSPLIT) {
+        int nch = box_split[si].n;
+        for (int c = 0; c < nch; ++c) {
+          int sb = bx.sb + c * KSPLIT, se = std::min(bx.se, sb + KSPLIT);
+          make_work(wbox, D.n_diff, bx, part_b + size_t(cur + c) * D.H, sb, se);
+        }
+        cur += nch;
+        ++si;
+      } else {
+        make_work(wbox, D.n_diff, bx, bx.out, bx.sb, bx.se);
+      }
+    }
+  }
+  NudftWork* d_work;
+  size_t nw = wroot.size() + wbox.size();
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_work), sizeof(NudftWork) * (nw + 1), st_));
+  std::vector<NudftWork> all(wbox);
+  all.insert(all.end(), wroot.begin(), wroot.end());
+  PDMK_CUDA(cudaMemcpyAsync(d_work, all.data(), sizeof(NudftWork) * nw, cudaMemcpyHostToDevice, st_));
+  time_begin(3);
+  dispatch_nudft(D.n_diff, d_work, int(wbox.size()), D, st_);
+  time_end(3);
+  dispatch_nudft(D.n_window, d_work + wbox.size(), int(wroot.size()), D, st_);
+  // reduce split-K chunks
+  auto reduce = [&](const std::vector<Chunked>& sp, const double2* pbase, int H) {
+    if (sp.empty()) return;
+    int nbx = int(sp.size());
+    std::vector<int> first(nbx), cntv(nbx);
+    std::vector<double2*> outs(nbx);
+    for (int i = 0; i < nbx; ++i) {
+      first[i] = sp[i].first;
+      cntv[i] = sp[i].n;
+      outs[i] = sp[i].out;
+    }
+    int* d_meta;
+    double2** d_outs;
+    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_meta), sizeof(int) * 2 * nbx + 16, st_));
+    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_outs), sizeof(double2*) * nbx + 16, st_));
+    PDMK_CUDA(cudaMemcpyAsync(d_meta, first.data(), sizeof(int) * nbx, cudaMemcpyHostToDevice, st_));
+    PDMK_CUDA(cudaMemcpyAsync(d_meta + nbx, cntv.data(), sizeof(int) * nbx, cudaMemcpyHostToDevice, st_));
+    PDMK_CUDA(cudaMemcpyAsync(d_outs, outs.data(), sizeof(double2*) * nbx, cudaMemcpyHostToDevice, st_));
+    dim3 grid(grid_for(H), unsigned(nbx));
+    k_reduce_chunks<<<grid, TPB, 0, st_>>>(pbase, d_meta, d_meta + nbx, d_outs, H);
+    PDMK_LAUNCH_CHECK();
+    PDMK_CUDA(cudaFreeAsync(d_meta, st_));
+    PDMK_CUDA(cudaFreeAsync(d_outs, st_));
+  };
+  reduce(root_split, part, D.Hw);
+  reduce(box_split, part_b, D.H);
+  PDMK_CUDA(cudaFreeAsync(d_work, st_));
+  PDMK_CUDA(cudaFreeAsync(part, st_));
+  diff_cached_ = false;
+}
+
+void DmkTree::prepare_box_lists() {
+  if (box_lists_ready_) return;
+  DevTree& D = dev_;
+  std::vector<int> c0(D.n_nodes);
+  PDMK_CUDA(cudaMemcpyAsync(c0.data(), D.node_child0, 4 * D.n_nodes, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  std::vector<int> nonleaf;
+  if (D.pw_hi >= D.pw_lo)
+    for (int id = D.level_start[D.pw_lo]; id < D.level_start[D.pw_hi + 1]; ++id)
+      if (c0[id] >= 0) nonleaf.push_back(id);
+  std::vector<int> leaves;
+  for (int id = D.level_start[2]; id < D.n_nodes; ++id)
+    if (c0[id] < 0) leaves.push_back(id);
+  n_nonleaf_ = int(nonleaf.size());
+  n_leaves_ = int(leaves.size());
+  d_nonleaf_ = static_cast<int*>(alloc(sizeof(int) * (n_nonleaf_ + 1)));
+  d_leaves_ = static_cast<int*>(alloc(sizeof(int) * (n_leaves_ + 1)));
+  PDMK_CUDA(cudaMemcpyAsync(d_nonleaf_, nonleaf.data(), sizeof(int) * n_nonleaf_, cudaMemcpyHostToDevice, st_));
+  PDMK_CUDA(cudaMemcpyAsync(d_leaves_, leaves.data(), sizeof(int) * n_leaves_, cudaMemcpyHostToDevice, st_));
+  // per-level constants of eval_energy_diff (src/energy.cpp:50-57)
+  const double pi = 3.14159265358979323846;
+  std::vector<double> Cl(MAX_LEVELS + 2, 0.0), Sl(MAX_LEVELS + 2, 0.0);
+  for (int l = 2; l < MAX_LEVELS + 1; ++l) {
+    Cl[l] = 1 / (2 * std::pow(2 * pi, 3)) * std::pow(D.delta_k[l], 3);
+    Sl[l] = ps_.psi0_0 * (1 / (2 * D.boxsize[l + 1] * ps_.C0) - 1 / (2 * D.boxsize[l] * ps_.C0));
+  }
+  d_Cl_ = static_cast<double*>(alloc(sizeof(double) * 2 * (MAX_LEVELS + 2)));
+  d_Sl_ = d_Cl_ + (MAX_LEVELS + 2);
+  PDMK_CUDA(cudaMemcpyAsync(d_Cl_, Cl.data(), sizeof(double) * (MAX_LEVELS + 2), cudaMemcpyHostToDevice, st_));
+  PDMK_CUDA(cudaMemcpyAsync(d_Sl_, Sl.data(), sizeof(double) * (MAX_LEVELS + 2), cudaMemcpyHostToDevice, st_));
+  d_scalars_ = static_cast<double*>(alloc(sizeof(double) * 8));
+  k_sum_q2<<<1, 1024, 0, st_>>>(D.sq, D.n_slots, d_scalars_ + 4);
+  PDMK_LAUNCH_CHECK();
+  PDMK_CUDA(cudaMemcpyAsync(&Q_, d_scalars_ + 4, sizeof(double), cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  box_lists_ready_ = true;
+}
+
+void DmkTree::run_incoming(bool write_inc) {
+  prepare_box_lists();
+  DevTree& D = dev_;
+  if (n_nonleaf_ == 0) {
+    PDMK_CUDA(cudaMemsetAsync(d_scalars_ + 1, 0, sizeof(double), st_));
+    return;
+  }
+  const int ktiles = (D.H + TPB - 1) / TPB;
+  double* part = D.partials;
+  double* q2 = D.partials + size_t(ktiles) * n_nonleaf_;
+  if (write_inc) {
+    k_incoming<<<unsigned(ktiles * n_nonleaf_), TPB, 0, st_>>>(D, d_nonleaf_, n_nonleaf_, 1, part);
+  } else {
+    k_tridot<<<unsigned(ktiles * n_nonleaf_), TPB, 0, st_>>>(D, d_nonleaf_, n_nonleaf_, part);
+  }
+  PDMK_LAUNCH_CHECK();
+  k_box_q2<<<unsigned(n_nonleaf_), TPB, 0, st_>>>(D, d_nonleaf_, q2);
+  PDMK_LAUNCH_CHECK();
+  k_diff_finish<<<1, 1024, 0, st_>>>(D, d_nonleaf_, n_nonleaf_, ktiles, part, q2, d_Cl_, d_Sl_, d_scalars_ + 1);
+  PDMK_LAUNCH_CHECK();
+}
+
+void DmkTree::form_incoming_pw() {
+  run_incoming(true);
+  diff_cached_ = true;
+}
+
+double DmkTree::eval_window_energy() {
+  prepare_box_lists();
+  DevTree& D = dev_;
+  const double pi = 3.14159265358979323846;
+  double scale = 1 / (2 * std::pow(2 * pi, 3)) * std::pow(D.delta_k[0], 3);
+  double self = Q_ * ps_.psi0_0 / (2 * D.boxsize[2] * ps_.C0);
+  k_window<<<1, 1024, 0, st_>>>(D, scale, self, d_scalars_ + 0);
+  PDMK_LAUNCH_CHECK();
+  double e;
+  PDMK_CUDA(cudaMemcpyAsync(&e, d_scalars_ + 0, sizeof(double), cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  return e;
+}
+
+double DmkTree::eval_diff_energy() {
+  if (!diff_cached_) run_incoming(false);
+  double e;
+  PDMK_CUDA(cudaMemcpyAsync(&e, d_scalars_ + 1, sizeof(double), cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  return e;
+}
+
+double DmkTree::eval_res_energy() {
+  ensure_packed();
+  prepare_box_lists();
+  DevTree& D = dev_;
+  if (n_leaves_ > 0) {
+    k_residual<<<unsigned(n_leaves_), RES_T, 0, st_>>>(D, d_leaves_, D.partials);
+    PDMK_LAUNCH_CHECK();
+    k_sum<<<1, 1024, 0, st_>>>(D.partials, n_leaves_, d_scalars_ + 2);
+    PDMK_LAUNCH_CHECK();
+  }
+  double e = 0;
+  PDMK_CUDA(cudaMemcpyAsync(&e, d_scalars_ + 2, sizeof(double), cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  return e;
+}
+
+EnergyParts DmkTree::eval_energy() {
+  EnergyParts p;
+  p.window = eval_window_energy();
+  p.diff = eval_diff_energy();
+  p.res = eval_res_energy();
+  return p;
+}
+
+}  // namespace pdmk

@@ -1,0 +1,224 @@
+// The device-resident DMK tree behind the C-ABI: particles binned into a
+// periodic 2:1-balanced adaptive octree, per-level plane-wave expansions, and
+// the kernels that form, evaluate and update them on one B200.
+//
+// Reference counterpart: struct HPDMKPtTree<Real> (include/tree.hpp:29-132)
+// and its methods in src/tree.cpp, src/planewave.cpp, src/energy.cpp and
+// src/energy_shift.cpp.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "pswf.hpp"
+
+namespace pdmk {
+
+constexpr int MAX_POLY = 25;
+constexpr int PATH_LEN_MAX = MAX_LEVELS;
+
+// One proposed single-particle move and what the shift kernel found for it.
+struct Proposal {
+  int i_orig;
+  int slot;       // current slot (>= n_slots: overflow pool entry)
+  double q;
+  double xo[3], xt[3];
+  int depth_o, depth_t;  // number of path nodes (leaf level + 1)
+  int path_o[PATH_LEN_MAX], path_t[PATH_LEN_MAX];
+  double dE;
+  double parts[5];  // window, difference, residual(target), residual(origin), self
+  int accepted;
+  int valid;
+};
+
+// Everything the kernels need, by value (all pointers are device pointers).
+struct DevTree {
+  double L;
+  int N;
+  int n_window, n_diff;
+  int dw, dd;  // 2n+1
+  int Hw, H;   // half-space sizes d^2 (n+1)
+  int max_depth;  // number of levels
+  int n_nodes;
+  int level_start[MAX_LEVELS + 2];
+  double boxsize[MAX_LEVELS + 2];
+  double delta_k[MAX_LEVELS + 2];
+  double dscale[MAX_LEVELS + 2];  // D_l = D_2 * dscale[l]
+  int pw_lo, pw_hi;               // levels carrying expansions: [pw_lo, pw_hi]
+  double poly[MAX_POLY];
+  int n_poly;
+  // particle slots (leaf-major in Morton order, with slack)
+  int n_slots;
+  double *sx, *sy, *sz, *sq;
+  int* s_orig;     // original index or -1
+  int* orig_slot;  // [N]; values >= n_slots are pool entries
+  // overflow pool for arrivals into full leaves
+  int pool_cap;
+  double *px, *py, *pz, *pq;
+  int *p_orig, *p_leaf;
+  int* pool_n;
+  // nodes (level-major, Morton order within a level)
+  uint64_t* node_prefix;
+  int* node_level;
+  int* node_parent;
+  int* node_child0;  // -1 for leaves
+  int* node_begin;   // slot range of the subtree
+  int* node_end;
+  int* leaf_count;  // particles present in a leaf (compact from node_begin)
+  int* node_count;  // particles in the subtree (maintained by moves)
+  int* col27;       // [n_nodes][27], same-level neighbours, -1 absent or self
+  int* coarse8;     // [n_nodes][8], coarse-grain leaf neighbours, -1 pad
+  // refinement bitmaps per level and exclusive word-popcount prefixes: the
+  // node id of any cell follows from these without walking the tree
+  const uint32_t* bm[MAX_LEVELS];
+  const int* wprefix[MAX_LEVELS];
+  int maxref;  // deepest level with a refined cell
+  // expansions: root, then nodes of levels [pw_lo, pw_hi] (contiguous ids)
+  double2* out_root;
+  double2* out;  // [(node - level_start[pw_lo]) * H + k]
+  double2* inc;
+  double* W;   // [Hw]
+  double* D2;  // [H], the level-2 difference kernel
+  // scratch
+  double* partials;
+  unsigned int* counter;
+  Proposal* prop;
+  int* err;  // device error word (nonzero: pool overflow etc.)
+  unsigned long long* work;  // [0] accepted moves, [1] update bytes (read + write)
+};
+
+struct EnergyParts {
+  double window = 0, diff = 0, res = 0;
+  double total() const { return window + diff + res; }
+};
+
+// positions in [0, L) and finite charges, checked on the device (synchronises)
+bool device_positions_valid(const double* d_r, const double* d_q, long n, double L, cudaStream_t st);
+
+struct TreeOptions {
+  int leaf_slack = 0;      // extra particle slots per leaf for moves
+  int pool_capacity = 4096;
+};
+
+class DmkTree {
+ public:
+  DmkTree(double L, int n_per_leaf, int digits, long n, const double* r, const double* q, bool inputs_on_device,
+          const TreeOptions& opt, cudaStream_t stream);
+  ~DmkTree();
+  DmkTree(const DmkTree&) = delete;
+  DmkTree& operator=(const DmkTree&) = delete;
+
+  void form_outgoing_pw();
+  void form_incoming_pw();
+  EnergyParts eval_energy();
+  double eval_window_energy();
+  double eval_diff_energy();
+  double eval_res_energy();
+  // single move through the drop-in API: host scalars in, host scalar out
+  double eval_shift_energy(long i, double dx, double dy, double dz, double* parts = nullptr);
+  void update_shift(long i, double dx, double dy, double dz);
+  // sequential Metropolis over device-resident proposals; no host sync
+  void mc_run_device(int n_moves, const int* d_idx, const double* d_disp, const double* d_u, double beta,
+                     double* d_dE, int* d_acc);
+  // batched energy shifts of many candidates against the current state
+  void shift_batch_device(int m, const int* d_idx, const double* d_disp, double* d_dE);
+
+  // introspection (tests)
+  int max_depth() const { return dev_.max_depth; }
+  int n_nodes() const { return dev_.n_nodes; }
+  const DevTree& dev() const { return dev_; }
+  void export_nodes(int* level, uint64_t* prefix, int* is_leaf, long* count) const;
+  void export_neighbors(int* col27, int* coarse8) const;
+  void export_sorted_order(long* orig_of_sorted) const;
+  void export_positions(double* r_orig_order) const;
+  void export_pw(long node, int which, double* out) const;
+  void export_W(double* out) const;
+  void export_D(int level, double* out) const;
+  void synchronize() const;
+  cudaStream_t stream() const { return st_; }
+  int check_device_error() const;
+  void repack(int leaf_slack);
+
+ private:
+  void build(const double* r, const double* q, bool on_device);
+  void build_setup();
+  void layout_slots(const double* dsx, const double* dsy, const double* dsz, const double* dsq, const int* dorig,
+                    const long* src_lo, int leaf_slack);
+  size_t partials_needed() const;
+  void launch_shift(const int* d_idx, const double* d_disp, const double* d_u, double beta, int move, int mode,
+                    double* d_dE, int* d_acc);
+  void launch_update();
+  void launch_commit();
+  void ensure_packed();
+  void prepare_box_lists();
+  void run_incoming(bool write_inc);
+
+  double L_;
+  int n_per_leaf_;
+  int digits_;
+  long N_;
+  TreeOptions opt_;
+  cudaStream_t st_;
+  ProlateSetup ps_;
+  DevTree dev_{};
+  // host copies of the topology
+  std::vector<int> h_level_start_;
+  std::vector<int> leaf_ids_;  // leaves in depth-first (Morton) order
+  std::vector<void*> allocs_;
+  void* alloc(size_t bytes);
+  // leaves in depth-first order and their slot bookkeeping (device)
+  struct LeafArrays {
+    int n = 0;
+    int* lid = nullptr;          // node id of the j-th leaf
+    int* cnt = nullptr;          // particles at layout time
+    int* cap = nullptr;          // slots
+    int* begin = nullptr;        // first slot
+    int* cnt_prefix = nullptr;   // exclusive prefix of cnt
+    int* dfs_of_node = nullptr;  // node id -> j (leaves only)
+  } leaf_dev_;
+  void* slot_block_ = nullptr;
+  int slot_capacity_ = 0;
+  size_t partials_cap_ = 0;
+  // energy bookkeeping
+  bool diff_cached_ = false;
+  bool box_lists_ready_ = false;
+  int n_nonleaf_ = 0, n_leaves_ = 0;
+  int* d_nonleaf_ = nullptr;  // non-leaf nodes of the expansion levels
+  int* d_leaves_ = nullptr;   // leaves at levels >= 2
+  double* d_Cl_ = nullptr;
+  double* d_Sl_ = nullptr;
+  double* d_scalars_ = nullptr;
+  double Q_ = 0;
+  // optional CUDA-event timing per kernel class (0 shift, 1 update pair, 2 commit, 3 NUDFT)
+ public:
+  void set_timing(bool on) { timing_ = on; }
+  void get_timing(double* out, bool reset);
+  void get_work(double* out);
+  void reset_work();
+  void time_begin(int cls);
+  void time_end(int cls);
+
+ private:
+  bool timing_ = false;
+  std::vector<cudaEvent_t> ev_pool_;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_open_;
+  double t_ms_[4] = {0, 0, 0, 0};
+  long t_cnt_[4] = {0, 0, 0, 0};
+  cudaEvent_t ev_cur_[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t take_event();
+  int shift_grid_ = 0;
+  int update_grid_ = 0;
+  // host-side copy of the last proposal arguments (for update_shift)
+  long last_i_ = -1;
+  double last_d_[3] = {0, 0, 0};
+  bool last_valid_ = false;
+  // arguments of the single-move API in device memory
+  int* d_one_idx_ = nullptr;
+  double* d_one_disp_ = nullptr;
+  double* d_one_u_ = nullptr;
+};
+
+}  // namespace pdmk

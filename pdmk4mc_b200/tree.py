@@ -1,0 +1,323 @@
+"""Python mirror of the reference's HPDMKPtTree<double> (include/tree.hpp:29-132)
+over the C-ABI of libhpdmk_b200.so (include/hpdmk.h).
+
+    params = HPDMKParams(n_per_leaf=10, digits=9, L=20.0, init=DIRECT)
+    tree = HPDMKPtTree(params, r_src, charge)    # r_src: [3n] xyz-interleaved in [0, L)
+    tree.form_outgoing_pw(); tree.form_incoming_pw()
+    E = tree.eval_energy()
+    dE = tree.eval_shift_energy(i, dx, dy, dz)
+    tree.update_shift(i, dx, dy, dz)
+
+Errors of the library (the reference's exceptions) raise HPDMKError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+DIRECT = 1
+PROXY = 2
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_lp = ctypes.POINTER(ctypes.c_long)
+_ip = ctypes.POINTER(ctypes.c_int)
+_ullp = ctypes.POINTER(ctypes.c_ulonglong)
+
+
+class HPDMKError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"hpdmk error {code}: {message}")
+        self.code = code
+
+
+class _Params(ctypes.Structure):
+    # include/hpdmk.h: struct HPDMKParams (same layout as the reference's)
+    _fields_ = [("n_per_leaf", ctypes.c_int), ("digits", ctypes.c_int), ("L", ctypes.c_double),
+                ("prolate_order", ctypes.c_double), ("init", ctypes.c_int)]
+
+
+class _ExtParams(ctypes.Structure):
+    _fields_ = [("leaf_slack", ctypes.c_int), ("pool_capacity", ctypes.c_int), ("precision", ctypes.c_int),
+                ("device", ctypes.c_int), ("stream", ctypes.c_void_p)]
+
+
+@dataclass
+class HPDMKParams:
+    """include/hpdmk.h:11-17 of the reference, with its defaults."""
+    n_per_leaf: int = 200
+    digits: int = 3
+    L: float = 1.0
+    prolate_order: float = 16
+    init: int = PROXY
+
+
+def library_path() -> str:
+    return os.environ.get("PDMK_B200_LIB", os.path.join(_HERE, "libhpdmk_b200.so"))
+
+
+def load_library():
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        raise ImportError(f"libhpdmk_b200.so not built: {path} (run __graft_entry__.build() or make -C "
+                          f"pdmk4mc_b200/csrc)")
+    L = ctypes.CDLL(path)
+    L.hpdmk_tree_create.restype = None
+    L.hpdmk_tree_create.argtypes = [ctypes.c_int, _Params, ctypes.c_int, _dp, _dp]
+    L.hpdmk_tree_init.restype = ctypes.c_void_p
+    L.hpdmk_tree_init.argtypes = [ctypes.c_int, _Params, ctypes.c_int, _dp, _dp]
+    L.hpdmk_tree_init_ext.restype = ctypes.c_void_p
+    L.hpdmk_tree_init_ext.argtypes = [ctypes.c_int, _Params, ctypes.POINTER(_ExtParams), ctypes.c_int, _dp, _dp]
+    L.hpdmk_tree_init_device.restype = ctypes.c_void_p
+    L.hpdmk_tree_init_device.argtypes = [ctypes.c_int, _Params, ctypes.POINTER(_ExtParams), ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_void_p]
+    L.hpdmk_get_stream.restype = ctypes.c_int
+    L.hpdmk_get_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    L.hpdmk_set_timing.restype = ctypes.c_int
+    L.hpdmk_set_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.hpdmk_get_timing.restype = ctypes.c_int
+    L.hpdmk_get_timing.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int]
+    L.hpdmk_get_update_bytes.restype = ctypes.c_int
+    L.hpdmk_get_update_bytes.argtypes = [ctypes.c_void_p, _dp]
+    L.hpdmk_tree_destroy.restype = None
+    L.hpdmk_tree_destroy.argtypes = [ctypes.c_void_p]
+    for name in ("hpdmk_form_outgoing_pw", "hpdmk_form_incoming_pw", "hpdmk_synchronize"):
+        getattr(L, name).restype = ctypes.c_int
+        getattr(L, name).argtypes = [ctypes.c_void_p]
+    L.hpdmk_eval_energy.restype = ctypes.c_int
+    L.hpdmk_eval_energy.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
+    L.hpdmk_energy.restype = ctypes.c_int
+    L.hpdmk_energy.argtypes = [ctypes.c_void_p, _dp]
+    L.hpdmk_eval_shift_energy.restype = ctypes.c_int
+    L.hpdmk_eval_shift_energy.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double, _dp]
+    L.hpdmk_debug_shift_parts.restype = ctypes.c_int
+    L.hpdmk_debug_shift_parts.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double, _dp]
+    L.hpdmk_update_shift.restype = ctypes.c_int
+    L.hpdmk_update_shift.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double]
+    L.hpdmk_eval_shift_energy_batch.restype = ctypes.c_int
+    L.hpdmk_eval_shift_energy_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp]
+    L.hpdmk_mc_run.restype = ctypes.c_int
+    L.hpdmk_mc_run.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp, ctypes.c_double, _dp, _ip]
+    L.hpdmk_mc_run_device.restype = ctypes.c_int
+    L.hpdmk_mc_run_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+    L.hpdmk_get_positions.restype = ctypes.c_int
+    L.hpdmk_get_positions.argtypes = [ctypes.c_void_p, _dp]
+    L.hpdmk_tree_info.restype = ctypes.c_int
+    L.hpdmk_tree_info.argtypes = [ctypes.c_void_p, _lp]
+    L.hpdmk_last_error.restype = ctypes.c_int
+    L.hpdmk_last_error.argtypes = []
+    L.hpdmk_last_error_message.restype = ctypes.c_char_p
+    L.hpdmk_last_error_message.argtypes = []
+    L.hpdmk_debug_nodes.restype = ctypes.c_int
+    L.hpdmk_debug_nodes.argtypes = [ctypes.c_void_p, _ip, _ullp, _ip, _lp]
+    L.hpdmk_debug_neighbors.restype = ctypes.c_int
+    L.hpdmk_debug_neighbors.argtypes = [ctypes.c_void_p, _ip, _ip]
+    L.hpdmk_debug_sorted_order.restype = ctypes.c_int
+    L.hpdmk_debug_sorted_order.argtypes = [ctypes.c_void_p, _lp]
+    L.hpdmk_debug_pw.restype = ctypes.c_int
+    L.hpdmk_debug_pw.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int, _dp]
+    L.hpdmk_debug_kernels.restype = ctypes.c_int
+    L.hpdmk_debug_kernels.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+    L.hpdmk_debug_prolate.restype = ctypes.c_int
+    L.hpdmk_debug_prolate.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _dp, _dp]
+    _LIB = L
+    return L
+
+
+def prolate_setup(digits: int, x=None):
+    """Host-side PSWF set-up of the library: (c, lambda, C0/psi0(0), diff0, n_window, n_diff), psi0(x)/psi0(0)."""
+    L = load_library()
+    out = np.zeros(6)
+    x = np.ascontiguousarray(np.zeros(0) if x is None else x, dtype=np.float64)
+    psi = np.zeros_like(x)
+    _check(L.hpdmk_debug_prolate(int(digits), _p(out), int(x.size), _p(x), _p(psi)))
+    return out, psi
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def _check(rc):
+    if rc != 0:
+        L = load_library()
+        raise HPDMKError(rc, L.hpdmk_last_error_message().decode(errors="replace"))
+
+
+class HPDMKPtTree:
+    """Device-resident DMK tree (reference: HPDMKPtTree<double>, include/tree.hpp:29-132)."""
+
+    def __init__(self, params: HPDMKParams, r_src, charge, leaf_slack: int = 8, pool_capacity: int = 4096,
+                 device: int = 0, stream=None, device_inputs=None):
+        """r_src / charge: host arrays; or, with device_inputs=(d_r_ptr, d_q_ptr, n), device pointers."""
+        L = load_library()
+        self.params = params
+        cp = _Params(int(params.n_per_leaf), int(params.digits), float(params.L), float(params.prolate_order),
+                     int(params.init))
+        ext = _ExtParams(int(leaf_slack), int(pool_capacity), 0, int(device), stream)
+        if device_inputs is not None:
+            d_r, d_q, n = device_inputs
+            self._h = L.hpdmk_tree_init_device(0, cp, ctypes.byref(ext), int(n), d_r, d_q)
+        else:
+            r = np.ascontiguousarray(r_src, dtype=np.float64).reshape(-1)
+            q = np.ascontiguousarray(charge, dtype=np.float64).reshape(-1)
+            if r.size != 3 * q.size:
+                raise ValueError("r_src must hold 3 coordinates per charge")
+            n = q.size
+            self._h = L.hpdmk_tree_init_ext(0, cp, ctypes.byref(ext), int(n), _p(r), _p(q))
+        if not self._h:
+            _check(L.hpdmk_last_error())
+        self.n = int(n)
+        self.L = float(params.L)
+        info = np.zeros(5, np.int64)
+        _check(L.hpdmk_tree_info(self._h, _p(info, _lp)))
+        self.max_depth, self.n_nodes, _, self.dims_window, self.dims_diff = (int(v) for v in info)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().hpdmk_tree_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def form_outgoing_pw(self):
+        _check(load_library().hpdmk_form_outgoing_pw(self._h))
+
+    def form_incoming_pw(self):
+        _check(load_library().hpdmk_form_incoming_pw(self._h))
+
+    def eval_energy_parts(self):
+        e, w, d, r = (ctypes.c_double() for _ in range(4))
+        _check(load_library().hpdmk_eval_energy(self._h, ctypes.byref(e), ctypes.byref(w), ctypes.byref(d),
+                                                ctypes.byref(r)))
+        return np.array([w.value, d.value, r.value])
+
+    def eval_energy(self) -> float:
+        return float(self.eval_energy_parts().sum())
+
+    def eval_energy_window(self):
+        return float(self.eval_energy_parts()[0])
+
+    def eval_energy_diff(self):
+        return float(self.eval_energy_parts()[1])
+
+    def eval_energy_res(self):
+        return float(self.eval_energy_parts()[2])
+
+    def eval_shift_energy(self, i, dx, dy, dz) -> float:
+        out = ctypes.c_double()
+        _check(load_library().hpdmk_eval_shift_energy(self._h, int(i), float(dx), float(dy), float(dz),
+                                                      ctypes.byref(out)))
+        return out.value
+
+    def eval_shift_energy_parts(self, i, dx, dy, dz):
+        """(window, difference, residual at target, residual at origin, self term)."""
+        p = np.zeros(5)
+        _check(load_library().hpdmk_debug_shift_parts(self._h, int(i), float(dx), float(dy), float(dz), _p(p)))
+        return p
+
+    def update_shift(self, i, dx, dy, dz):
+        _check(load_library().hpdmk_update_shift(self._h, int(i), float(dx), float(dy), float(dz)))
+
+    def eval_shift_energy_batch(self, idx, disp):
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        disp = np.ascontiguousarray(disp, dtype=np.float64).reshape(-1)
+        out = np.zeros(idx.size)
+        _check(load_library().hpdmk_eval_shift_energy_batch(self._h, int(idx.size), _p(idx, _lp), _p(disp),
+                                                            _p(out)))
+        return out
+
+    def mc_run(self, idx, disp, u, beta):
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        disp = np.ascontiguousarray(disp, dtype=np.float64).reshape(-1)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        dE = np.zeros(idx.size)
+        acc = np.zeros(idx.size, np.int32)
+        _check(load_library().hpdmk_mc_run(self._h, int(idx.size), _p(idx, _lp), _p(disp), _p(u), float(beta),
+                                           _p(dE), _p(acc, _ip)))
+        return dE, acc
+
+    def mc_run_device(self, n, d_idx_ptr, d_disp_ptr, d_u_ptr, beta, d_dE_ptr, d_acc_ptr):
+        _check(load_library().hpdmk_mc_run_device(self._h, int(n), d_idx_ptr, d_disp_ptr, d_u_ptr, float(beta),
+                                                  d_dE_ptr, d_acc_ptr))
+
+    def synchronize(self):
+        _check(load_library().hpdmk_synchronize(self._h))
+
+    def stream_ptr(self) -> int:
+        s = ctypes.c_void_p()
+        _check(load_library().hpdmk_get_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def set_timing(self, on: bool):
+        _check(load_library().hpdmk_set_timing(self._h, 1 if on else 0))
+
+    def get_timing(self, reset=False):
+        """{class: (total ms, launches)} for shift, update, commit and nudft kernels."""
+        o = np.zeros(8)
+        _check(load_library().hpdmk_get_timing(self._h, _p(o), 1 if reset else 0))
+        return {k: (o[2 * c], int(o[2 * c + 1])) for c, k in enumerate(("shift", "update", "commit", "nudft"))}
+
+    def update_work(self):
+        """(accepted moves, algorithmic update bytes) of the last MC batch."""
+        o = np.zeros(2)
+        _check(load_library().hpdmk_get_update_bytes(self._h, _p(o)))
+        return o
+
+    def positions(self):
+        r = np.zeros(3 * self.n)
+        _check(load_library().hpdmk_get_positions(self._h, _p(r)))
+        return r
+
+    # --- introspection for parity tests
+    def tree_nodes(self):
+        lv = np.zeros(self.n_nodes, np.int32)
+        pf = np.zeros(self.n_nodes, np.uint64)
+        lf = np.zeros(self.n_nodes, np.int32)
+        ct = np.zeros(self.n_nodes, np.int64)
+        _check(load_library().hpdmk_debug_nodes(self._h, _p(lv, _ip), _p(pf, _ullp), _p(lf, _ip), _p(ct, _lp)))
+        return lv, pf, lf, ct
+
+    def tree_neighbors(self):
+        col = np.zeros((self.n_nodes, 27), np.int32)
+        cg = np.zeros((self.n_nodes, 8), np.int32)
+        _check(load_library().hpdmk_debug_neighbors(self._h, _p(col, _ip), _p(cg, _ip)))
+        return col, cg
+
+    def sorted_order(self):
+        o = np.zeros(self.n, np.int64)
+        _check(load_library().hpdmk_debug_sorted_order(self._h, _p(o, _lp)))
+        return o
+
+    def pw(self, node, which="out"):
+        dims = self.dims_window if node == 0 else self.dims_diff
+        o = np.zeros(2 * dims)
+        _check(load_library().hpdmk_debug_pw(self._h, int(node), 0 if which == "out" else 1, _p(o)))
+        return o[0::2] + 1j * o[1::2]
+
+    def window_matrix(self):
+        o = np.zeros(self.dims_window)
+        _check(load_library().hpdmk_debug_kernels(self._h, 0, _p(o)))
+        return o
+
+    def difference_matrix(self, level):
+        o = np.zeros(self.dims_diff)
+        _check(load_library().hpdmk_debug_kernels(self._h, int(level), _p(o)))
+        return o

@@ -1,0 +1,93 @@
+"""CPU checks of the product boundary: the CUDA library loads, exports every
+entry point include/hpdmk.h declares, validates its inputs the way the
+reference does (errors instead of exceptions), and its host-side PSWF
+set-up matches the reference's golden vectors. No compute call needs a GPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import pdmk4mc_b200 as P
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+G = np.load(os.path.join(ROOT, "tests", "golden", "reference_math.npz"))
+
+
+def _declared_functions():
+    src = open(os.path.join(ROOT, "include", "hpdmk.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"\b(hpdmk_[a-z0-9_]+)\s*\(", src)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = P.load_library()
+    names = _declared_functions()
+    assert "hpdmk_tree_create" in names and "hpdmk_eval_shift_energy" in names
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_params_struct_layout_matches_reference():
+    # int, int, double, double, enum(int) -> 32 bytes, as the reference's struct
+    assert ctypes.sizeof(P.tree._Params) == 32
+    assert P.tree._Params.L.offset == 8 and P.tree._Params.init.offset == 24
+    d = P.HPDMKParams()
+    assert (d.n_per_leaf, d.digits, d.prolate_order, d.init) == (200, 3, 16, P.PROXY)
+
+
+@pytest.mark.parametrize("kw,code", [
+    (dict(digits=5), 1),                      # unsupported digits (src/tree.cpp:25-28)
+    (dict(digits=9, init=P.PROXY), 1),        # PROXY above 3 digits (src/upward_pass.cpp:9-14)
+    (dict(L=-1.0), 1),
+    (dict(n_per_leaf=0), 1),
+])
+def test_bad_params_rejected(kw, code):
+    base = dict(n_per_leaf=10, digits=6, L=10.0, init=P.DIRECT)
+    base.update(kw)
+    r = np.full(30, 1.0)
+    q = np.ones(10)
+    with pytest.raises(P.HPDMKError) as e:
+        P.HPDMKPtTree(P.HPDMKParams(**base), r, q)
+    assert e.value.code == code
+
+
+@pytest.mark.parametrize("bad", ["outside", "negative", "nan_q"])
+def test_bad_inputs_rejected(bad):
+    r = np.full(30, 1.0)
+    q = np.ones(10)
+    if bad == "outside":
+        r[4] = 10.0
+    elif bad == "negative":
+        r[7] = -1e-9
+    else:
+        q[3] = np.nan
+    with pytest.raises(P.HPDMKError) as e:
+        P.HPDMKPtTree(P.HPDMKParams(n_per_leaf=10, digits=6, L=10.0, init=P.DIRECT), r, q)
+    assert e.value.code == 2
+
+
+def test_reference_c_entry_point_is_safe_on_bad_input():
+    lib = P.load_library()
+    cp = P.tree._Params(10, 7, 10.0, 16.0, P.DIRECT)
+    r = np.full(30, 1.0)
+    q = np.ones(10)
+    lib.hpdmk_tree_create(0, cp, 10, r.ctypes.data_as(P.tree._dp), q.ctypes.data_as(P.tree._dp))
+    assert lib.hpdmk_last_error() == 1
+
+
+@pytest.mark.parametrize("digits", [3, 6, 9, 12])
+def test_host_prolate_setup_matches_reference(digits):
+    xs = G[f"d{digits}_psi0_x"]
+    out, psi = P.prolate_setup(digits, xs)
+    c, lam, c0r, diff0, nw, nd = out
+    assert c == G[f"d{digits}_c"]
+    assert int(nd) == int(G[f"d{digits}_n_diff"])
+    assert int(nw) == int(np.floor(2 * c / np.pi))
+    assert abs(lam / G[f"d{digits}_lambda"] - 1) < 1e-12
+    p0 = G[f"d{digits}_psi0"][0]
+    assert abs(c0r - G[f"d{digits}_C0"] / p0) < 1e-13
+    assert abs(diff0 / G[f"d{digits}_diff0"] - 1) < 1e-12
+    np.testing.assert_allclose(psi, G[f"d{digits}_psi0"] / p0, rtol=0, atol=1e-14)
