@@ -405,11 +405,25 @@ bool device_positions_valid(const double* d_r, const double* d_q, long n, double
 }
 
 // ---------------------------------------------------------------------------
+// Tree-lifetime allocations come from the device's stream-ordered pool, kept
+// cached across trees (the release threshold is raised once per device), so
+// building a fresh tree per full-energy evaluation costs no driver
+// allocations in steady state.
 void* DmkTree::alloc(size_t bytes) {
+  static bool pool_ready[64] = {false};
+  int dev = 0;
+  PDMK_CUDA(cudaGetDevice(&dev));
+  if (dev < 64 && !pool_ready[dev]) {
+    cudaMemPool_t pool;
+    PDMK_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t thr = ~uint64_t(0);
+    PDMK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    pool_ready[dev] = true;
+  }
   void* p = nullptr;
   if (bytes == 0) bytes = 16;
-  cudaError_t e = cudaMalloc(&p, bytes);
-  if (e != cudaSuccess) throw CudaError(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  cudaError_t e = cudaMallocAsync(&p, bytes, st_);
+  if (e != cudaSuccess) throw CudaError(std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
   allocs_.push_back(p);
   return p;
 }
@@ -423,9 +437,9 @@ DmkTree::DmkTree(double L, int n_per_leaf, int digits, long n, const double* r, 
     build_setup();
   } catch (...) {
     cudaStreamSynchronize(st_);
-    for (void* p : allocs_) cudaFree(p);
+    for (void* p : allocs_) cudaFreeAsync(p, st_);
     allocs_.clear();
-    if (slot_block_) cudaFree(slot_block_);
+    if (slot_block_) cudaFreeAsync(slot_block_, st_);
     slot_block_ = nullptr;
     throw;
   }
@@ -433,8 +447,22 @@ DmkTree::DmkTree(double L, int n_per_leaf, int digits, long n, const double* r, 
 
 DmkTree::~DmkTree() {
   cudaStreamSynchronize(st_);
-  for (void* p : allocs_) cudaFree(p);
-  if (slot_block_) cudaFree(slot_block_);
+  if (aux_) {
+    cudaStreamSynchronize(aux_);
+    cudaStreamDestroy(aux_);
+    cudaEventDestroy(ev_fork_);
+    cudaEventDestroy(ev_join_);
+  }
+  for (auto& gx : mc_graph_)
+    if (gx) cudaGraphExecDestroy(gx);
+  for (cudaEvent_t e : graph_ev_) cudaEventDestroy(e);
+  for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
+  for (auto& o : ev_open_) {
+    cudaEventDestroy(o.second.first);
+    cudaEventDestroy(o.second.second);
+  }
+  for (void* p : allocs_) cudaFreeAsync(p, st_);
+  if (slot_block_) cudaFreeAsync(slot_block_, st_);
 }
 
 void DmkTree::synchronize() const { PDMK_CUDA(cudaStreamSynchronize(st_)); }
@@ -686,11 +714,17 @@ void DmkTree::layout_slots(const double* dsx, const double* dsy, const double* d
   PDMK_CUDA(cudaMemcpyAsync(&last_cap, leaf_dev_.cap + nl - 1, 4, cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaStreamSynchronize(st_));
   const int n_slots = last_begin + last_cap;
+  // captured graphs hold the tree description by value: rebuild them later
+  for (auto& gx : mc_graph_)
+    if (gx) {
+      PDMK_CUDA(cudaGraphExecDestroy(gx));
+      gx = nullptr;
+    }
   if (n_slots > slot_capacity_) {
     // slot arrays live outside allocs_ so they can be regrown
-    if (slot_block_) cudaFree(slot_block_);
+    if (slot_block_) cudaFreeAsync(slot_block_, st_);
     slot_capacity_ = n_slots + n_slots / 8 + 64;
-    PDMK_CUDA(cudaMalloc(&slot_block_, size_t(slot_capacity_) * (4 * sizeof(double) + sizeof(int))));
+    PDMK_CUDA(cudaMallocAsync(&slot_block_, size_t(slot_capacity_) * (4 * sizeof(double) + sizeof(int)), st_));
   }
   double* base = static_cast<double*>(slot_block_);
   D.sx = base;
@@ -787,17 +821,23 @@ void DmkTree::build_setup() {
   D.pw_lo = 2;
   D.pw_hi = D.max_depth - 2;  // may be < pw_lo: no difference levels
   // window_matrix (include/kernels.hpp:60-86)
+  // The kernels depend on a mode only through m = ix^2 + iy^2 + iz^2 (in units
+  // of dk), so psi_0 is evaluated once per distinct m.
   std::vector<double> W(D.Hw);
   {
     int nk = s.n_window, d = D.dw;
     double dk = D.delta_k[1], sigma = sig[2];
+    std::vector<double> memo(3 * nk * nk + 1, std::nan(""));
     for (int k = 0; k < nk + 1; ++k)
       for (int j = 0; j < d; ++j)
         for (int i = 0; i < d; ++i) {
-          double kx = (i - nk) * dk, ky = (j - nk) * dk, kz = (k - nk) * dk;
-          double k2 = kx * kx + ky * ky + kz * kz;
-          double val = k2 != 0 ? s.fourier(std::sqrt(k2) * sigma) / k2 : 0.0;
-          W[(k * d + j) * d + i] = (k == nk) ? val : 2 * val;
+          int m = (i - nk) * (i - nk) + (j - nk) * (j - nk) + (k - nk) * (k - nk);
+          if (std::isnan(memo[m])) {
+            double kx = (i - nk) * dk, ky = (j - nk) * dk, kz = (k - nk) * dk;
+            double k2 = kx * kx + ky * ky + kz * kz;
+            memo[m] = k2 != 0 ? s.fourier(std::sqrt(k2) * sigma) / k2 : 0.0;
+          }
+          W[(k * d + j) * d + i] = (k == nk) ? memo[m] : 2 * memo[m];
         }
   }
   // difference_matrix at level 2 (include/kernels.hpp:88-114); every other
@@ -806,19 +846,22 @@ void DmkTree::build_setup() {
   {
     int nk = s.n_diff, d = D.dd;
     double dk = D.delta_k[2], sl = sig[2], slp1 = sig[3];
+    std::vector<double> memo(3 * nk * nk + 1, std::nan(""));
     for (int k = 0; k < nk + 1; ++k)
       for (int j = 0; j < d; ++j)
         for (int i = 0; i < d; ++i) {
-          double kx = (i - nk) * dk, ky = (j - nk) * dk, kz = (k - nk) * dk;
-          double k2 = kx * kx + ky * ky + kz * kz;
-          double val;
-          if (k2 == 0) {
-            val = s.diff0 * (slp1 * slp1 - sl * sl);
-          } else {
-            double kk = std::sqrt(k2);
-            val = (s.fourier(kk * slp1) - s.fourier(kk * sl)) / k2;
+          int m = (i - nk) * (i - nk) + (j - nk) * (j - nk) + (k - nk) * (k - nk);
+          if (std::isnan(memo[m])) {
+            double kx = (i - nk) * dk, ky = (j - nk) * dk, kz = (k - nk) * dk;
+            double k2 = kx * kx + ky * ky + kz * kz;
+            if (k2 == 0) {
+              memo[m] = s.diff0 * (slp1 * slp1 - sl * sl);
+            } else {
+              double kk = std::sqrt(k2);
+              memo[m] = (s.fourier(kk * slp1) - s.fourier(kk * sl)) / k2;
+            }
           }
-          D2[(k * d + j) * d + i] = (k == nk) ? val : 2 * val;
+          D2[(k * d + j) * d + i] = (k == nk) ? memo[m] : 2 * memo[m];
         }
   }
   D.W = static_cast<double*>(alloc(sizeof(double) * D.Hw));
@@ -841,6 +884,7 @@ void DmkTree::build_setup() {
   PDMK_CUDA(cudaMemsetAsync(D.counter, 0, 64, st_));
   D.prop = static_cast<Proposal*>(alloc(sizeof(Proposal)));
   PDMK_CUDA(cudaMemsetAsync(D.prop, 0, sizeof(Proposal), st_));
+  D.recv = static_cast<Receiver*>(alloc(sizeof(Receiver) * MAX_RECV));
   d_one_idx_ = static_cast<int*>(alloc(64));
   d_one_disp_ = static_cast<double*>(alloc(64));
   d_one_u_ = static_cast<double*>(alloc(64));

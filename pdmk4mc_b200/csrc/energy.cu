@@ -51,19 +51,22 @@ struct NudftWork {
   double2* out;       // H complex outputs of this box (or of this split-K chunk)
 };
 
+// Each thread owns one (kz, ky) row and TC <= 20 of its kx columns: 4 TC FP64
+// accumulators stay in registers (wider tiles spill), and the row factor
+// q ez ey costs one complex multiply per TC multiply-adds.
 template <int NK>
 struct NudftShape {
   static constexpr int D = 2 * NK + 1;
-  static constexpr int CG = D > 40 ? 2 : 1;           // column groups per row
+  static constexpr int CG = (D + 19) / 20;            // column groups per row
   static constexpr int TC = (D + CG - 1) / CG;        // columns per thread
   static constexpr int DP = TC * CG;                  // padded row stride in smem
   static constexpr int ROWS = (NK + 1) * D;
   static constexpr int WORK = ROWS * CG;              // thread tasks per box
-  static constexpr int TMAX = D > 30 ? 288 : 352;
+  static constexpr int TMAX = 512;
   static constexpr int TILES = (WORK + TMAX - 1) / TMAX;
   static constexpr int THREADS = ((WORK + TILES - 1) / TILES + 31) / 32 * 32;
-  static constexpr int KC = 16;                       // particles per shared-memory chunk
-  static constexpr int SMEM = KC * (2 * DP + NK + 1) * int(sizeof(double2));
+  static constexpr int KC = 32;                       // particles per shared-memory chunk
+  static constexpr int SMEM = 2 * KC * (2 * DP + NK + 1) * int(sizeof(double2));  // double-buffered
 };
 
 // per-axis factors exp(-i m dk (x - c)) * w6^{-M (2X+1) m}, m = m0 .. m0+cnt-1
@@ -87,10 +90,8 @@ __global__ void __launch_bounds__(NudftShape<NK>::THREADS)
     k_nudft(const NudftWork* __restrict__ work, const double* __restrict__ sx, const double* __restrict__ sy,
             const double* __restrict__ sz, const double* __restrict__ sq) {
   using S = NudftShape<NK>;
+  constexpr int BUF = S::KC * (2 * S::DP + NK + 1);  // complex entries per table buffer
   extern __shared__ double2 smem[];
-  double2* ex = smem;                    // [KC][DP]
-  double2* ey = ex + S::KC * S::DP;      // [KC][DP]
-  double2* ez = ey + S::KC * S::DP;      // [KC][NK+1], charge folded in
   const NudftWork w = work[blockIdx.x];
   const int g = w.row_tile * S::THREADS + threadIdx.x;
   const bool active = g < S::WORK;
@@ -98,17 +99,17 @@ __global__ void __launch_bounds__(NudftShape<NK>::THREADS)
   const int cg = active ? g % S::CG : 0;
   const int kz = row / S::D, ky = row % S::D;
   const int c0 = cg * S::TC;
-  double2 acc[S::TC];
-#pragma unroll
-  for (int c = 0; c < S::TC; ++c) acc[c] = make_double2(0.0, 0.0);
-  for (int base = w.s_begin; base < w.s_end; base += S::KC) {
+  // factor tables of one particle chunk: ex [KC][DP], ey [KC][DP], ez [KC][NK+1]
+  // (charge folded into ez); two buffers so the next chunk's tables are
+  // built while the current chunk is contracted (one barrier per chunk)
+  auto build = [&](int base, double2* buf) {
+    double2* ex = buf;
+    double2* ey = ex + S::KC * S::DP;
+    double2* ez = ey + S::KC * S::DP;
     const int nk = min(S::KC, w.s_end - base);
-    __syncthreads();
-    // factor tables: (particle, axis, half) tasks
     for (int t = threadIdx.x; t < S::KC * 6; t += blockDim.x) {
       int j = t / 6, a = (t / 2) % 3, half = t & 1;
       if (j >= nk) {
-        // zero rows so the inner loop needs no bound
         double2* dst = a == 0 ? ex + j * S::DP : (a == 1 ? ey + j * S::DP : ez + j * (NK + 1));
         int len = a == 2 ? NK + 1 : S::DP;
         for (int u = half; u < len; u += 2) dst[u] = make_double2(0.0, 0.0);
@@ -131,22 +132,41 @@ __global__ void __launch_bounds__(NudftShape<NK>::THREADS)
         axis_factors(sz[s] - w.cz, w.dk, w.M, w.Z, m0, cnt, sq[s], ez + j * (NK + 1) + (m0 + NK));
       }
     }
-    __syncthreads();
+  };
+  double2 acc[S::TC];
+#pragma unroll
+  for (int c = 0; c < S::TC; ++c) acc[c] = make_double2(0.0, 0.0);
+  if (w.s_begin < w.s_end) build(w.s_begin, smem);
+  __syncthreads();
+  int cur = 0;
+  for (int base = w.s_begin; base < w.s_end; base += S::KC) {
+    if (base + S::KC < w.s_end) build(base + S::KC, smem + (cur ^ 1) * BUF);
+    const double2* ex = smem + cur * BUF;
+    const double2* ey = ex + S::KC * S::DP;
+    const double2* ez = ey + S::KC * S::DP;
+    const int nk = min(S::KC, w.s_end - base);
     if (active) {
 #pragma unroll 2
       for (int j = 0; j < nk; ++j) {
         const double2 a = cmul(ez[j * (NK + 1) + kz], ey[j * S::DP + ky]);
         const double2* xr = ex + j * S::DP + c0;
+        // two sweeps keep the two FMAs of each complex product independent
 #pragma unroll
         for (int c = 0; c < S::TC; ++c) {
           const double2 b = xr[c];
           acc[c].x = fma(a.x, b.x, acc[c].x);
-          acc[c].x = fma(-a.y, b.y, acc[c].x);
           acc[c].y = fma(a.x, b.y, acc[c].y);
+        }
+#pragma unroll
+        for (int c = 0; c < S::TC; ++c) {
+          const double2 b = xr[c];
+          acc[c].x = fma(-a.y, b.y, acc[c].x);
           acc[c].y = fma(a.y, b.x, acc[c].y);
         }
       }
     }
+    __syncthreads();
+    cur ^= 1;
   }
   if (active) {
     double2* o = w.out + size_t(row) * S::D + c0;
@@ -427,7 +447,8 @@ __global__ void k_sum_q2(const double* sq, int n, double* out) {
 // ---------------------------------------------------------------------------
 // host side
 
-constexpr int KSPLIT = 4096;  // particles per split-K chunk
+constexpr int KSPLIT = 4096;       // particles per split-K chunk of a box
+constexpr int KSPLIT_ROOT = 2048;  // particles per chunk of the root pass
 
 size_t DmkTree::partials_needed() const {
   const DevTree& D = dev_;
@@ -501,7 +522,7 @@ void DmkTree::form_outgoing_pw() {
   };
   // root over all slots
   {
-    int nch = std::max(1, (D.n_slots + KSPLIT - 1) / KSPLIT);
+    int nch = std::max(1, (D.n_slots + KSPLIT_ROOT - 1) / KSPLIT_ROOT);
     root_split.push_back({0, nch, D.out_root});
     part_root = long(nch) * D.Hw;
   }
@@ -529,7 +550,7 @@ void DmkTree::form_outgoing_pw() {
     Box r{0, 0, D.n_slots, 0, D.out_root};
     int nch = root_split[0].n;
     for (int c = 0; c < nch; ++c) {
-      int sb = c * KSPLIT, se = std::min(D.n_slots, sb + KSPLIT);
+      int sb = c * KSPLIT_ROOT, se = std::min(D.n_slots, sb + KSPLIT_ROOT);
       make_work(wroot, D.n_window, r, part + size_t(c) * D.Hw, sb, se);
     }
   }
@@ -558,10 +579,20 @@ void DmkTree::form_outgoing_pw() {
   std::vector<NudftWork> all(wbox);
   all.insert(all.end(), wroot.begin(), wroot.end());
   PDMK_CUDA(cudaMemcpyAsync(d_work, all.data(), sizeof(NudftWork) * nw, cudaMemcpyHostToDevice, st_));
+  // the root pass (few CTAs) overlaps the box pass on a second stream
+  if (!aux_) {
+    PDMK_CUDA(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking));
+    PDMK_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+    PDMK_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
+  }
+  PDMK_CUDA(cudaEventRecord(ev_fork_, st_));
+  PDMK_CUDA(cudaStreamWaitEvent(aux_, ev_fork_, 0));
+  dispatch_nudft(D.n_window, d_work + wbox.size(), int(wroot.size()), D, aux_);
+  PDMK_CUDA(cudaEventRecord(ev_join_, aux_));
   time_begin(3);
   dispatch_nudft(D.n_diff, d_work, int(wbox.size()), D, st_);
   time_end(3);
-  dispatch_nudft(D.n_window, d_work + wbox.size(), int(wroot.size()), D, st_);
+  PDMK_CUDA(cudaStreamWaitEvent(st_, ev_join_, 0));
   // reduce split-K chunks
   auto reduce = [&](const std::vector<Chunked>& sp, const double2* pbase, int H) {
     if (sp.empty()) return;
@@ -632,6 +663,7 @@ void DmkTree::prepare_box_lists() {
 }
 
 void DmkTree::run_incoming(bool write_inc) {
+  ensure_packed();
   prepare_box_lists();
   DevTree& D = dev_;
   if (n_nonleaf_ == 0) {
@@ -673,6 +705,7 @@ double DmkTree::eval_window_energy() {
 }
 
 double DmkTree::eval_diff_energy() {
+  ensure_packed();
   if (!diff_cached_) run_incoming(false);
   double e;
   PDMK_CUDA(cudaMemcpyAsync(&e, d_scalars_ + 1, sizeof(double), cudaMemcpyDeviceToHost, st_));
@@ -697,6 +730,9 @@ double DmkTree::eval_res_energy() {
 }
 
 EnergyParts DmkTree::eval_energy() {
+  // per-box charge sums and the near field read particles from the slot
+  // ranges: fold any overflow-pool arrivals back into them first
+  ensure_packed();
   EnergyParts p;
   p.window = eval_window_energy();
   p.diff = eval_diff_energy();

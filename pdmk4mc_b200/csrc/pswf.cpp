@@ -9,6 +9,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 
 namespace pdmk {
@@ -160,7 +162,24 @@ double ProlateSetup::psi0(double x) const {
   return legendre_series(legendre, x);
 }
 
+namespace {
+ProlateSetup compute_prolate_setup(int digits);
+}
+
+// one set-up per digits setting per process
 ProlateSetup make_prolate_setup(int digits) {
+  static std::mutex mu;
+  static std::map<int, ProlateSetup> cache;
+  std::lock_guard<std::mutex> g(mu);
+  auto it = cache.find(digits);
+  if (it != cache.end()) return it->second;
+  ProlateSetup s = compute_prolate_setup(digits);
+  cache[digits] = s;
+  return s;
+}
+
+namespace {
+ProlateSetup compute_prolate_setup(int digits) {
   const TableRow* row = nullptr;
   for (const auto& r : table())
     if (r.digits == digits) row = &r;
@@ -190,5 +209,6 @@ ProlateSetup make_prolate_setup(int digits) {
   s.diff0 = -2.0 * kPi * x2 / c0 * s.c * s.c;
   return s;
 }
+}  // namespace
 
 }  // namespace pdmk

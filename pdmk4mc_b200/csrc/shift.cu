@@ -6,12 +6,16 @@
 // (src/tree.cpp:204-236), form_outgoing_pw_single (src/planewave.cpp:157-181)
 // and update_shift (src/tree.cpp:447-597).
 //
-// One trial move runs as: k_shift (grid-wide partial sums, the last block
-// finishes dE and the Metropolis test and writes the Proposal record),
-// k_update for the target path and then for the origin path (the two never
-// race on a vector), and k_commit (particle membership). Every kernel reads
-// the Proposal record, so the whole sequence is stream-ordered and can be
-// captured in a CUDA graph.
+// One trial move runs as: k_shift (grid-wide partial sums; the last block
+// finishes dE and the Metropolis test, lists the expansion vectors an
+// accepted move changes and writes the Proposal record), then k_update (one
+// read-modify-write per touched vector, target and origin contributions
+// merged; block 0 also commits the particle membership). Both kernels read
+// the Proposal record, so the sequence is stream-ordered and can be captured
+// in a CUDA graph. Per-move latency is what bounds Monte Carlo throughput,
+// so the kernels avoid dependent global loads: box coordinates along both
+// paths come from the particle's grid key, the 27 minimum-image candidates
+// and the two paths are resolved by the lanes of one warp in parallel.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -32,38 +36,18 @@ __device__ inline int bm_rank(const DevTree& T, int level, uint64_t cell) {
   return T.wprefix[level][cell >> 5] + __popc(w & ((1u << (cell & 31)) - 1u));
 }
 
-// Leaf path of a point: lane l resolves level l from the refinement bitmaps.
-// Must be called by a full warp; returns the path length (leaf level + 1).
-__device__ inline int warp_path(const DevTree& T, double x, double y, double z, int* path) {
-  const int lane = threadIdx.x & 31;
-  const uint64_t key = morton3(grid_coord(x, T.L), grid_coord(y, T.L), grid_coord(z, T.L));
-  bool is_leaf = false;
-  int node = -1;
-  if (lane < T.max_depth) {
-    const int l = lane;
-    const uint64_t cell = l == 0 ? 0 : key >> (3 * (KEY_BITS - l));
-    bool exists = l <= 1 || bm_get(T.bm[l - 1], cell >> 3);
-    if (exists) {
-      node = l == 0 ? 0 : (l == 1 ? 1 + int(cell) : T.level_start[l] + 8 * bm_rank(T, l - 1, cell >> 3) + int(cell & 7));
-      bool refined = l <= T.maxref && bm_get(T.bm[l], cell);
-      is_leaf = !refined;
-    }
-  }
-  unsigned leaves = __ballot_sync(0xffffffffu, is_leaf);
-  int leaf_level = __ffs(leaves) - 1;
-  if (lane <= leaf_level) path[lane] = node;
-  __syncwarp();
-  return leaf_level + 1;
+__device__ inline double center_of(double L, int l, int X) {
+  double scale = ldexp(1.0, -l);
+  return L * (double(X) * scale + 0.5 * scale);
 }
 
 __device__ inline void node_center(const DevTree& T, int node, double* c, int* X) {
-  uint64_t p = T.node_prefix[node];
-  int l = T.node_level[node];
-  double scale = ldexp(1.0, -l);
+  const uint64_t p = T.node_prefix[node];
+  const int l = T.node_level[node];
   X[0] = int(compact3(p));
   X[1] = int(compact3(p >> 1));
   X[2] = int(compact3(p >> 2));
-  for (int d = 0; d < 3; ++d) c[d] = T.L * (double(X[d]) * scale + 0.5 * scale);
+  for (int d = 0; d < 3; ++d) c[d] = center_of(T.L, l, X[d]);
 }
 
 __device__ inline int periodic_shift_d(double xi, double xj, double L, double bi, double bj) {
@@ -80,13 +64,28 @@ __device__ inline double poly_res(const DevTree& T, double r, double b) {
   return v / r;
 }
 
-// Phase tables exp(-i m dk_l x) per axis for one point on its path: slot 0
-// is the root (window modes), slot l (2 <= l <= pw_hi) the level-l box on the
-// path. The box-centred form uses the exact decentring root of unity.
+// Phase tables exp(-i m dk_l x) per axis for one point on its path. Layout:
+// root axes (3 x dw), then levels 2, 3, ... (3 x dd each). The accessors
+// compute addresses, so no pointer array is indexed at run time.
 struct Tables {
-  double2* root[3];
-  double2* lev[MAXLV + 2][3];
+  struct Axes {
+    double2* b;
+    int stride;
+    __device__ double2* operator[](int ax) const { return b + ax * stride; }
+  };
+  struct Levels {
+    double2* b;
+    int dw, dd;
+    __device__ Axes operator[](int l) const { return Axes{b + 3 * dw + (l - 2) * 3 * dd, dd}; }
+  };
+  Axes root;
+  Levels lev;
 };
+
+__device__ inline void alloc_tables(double2* sm, const DevTree& T, Tables& tb) {
+  tb.root = Tables::Axes{sm, 2 * T.n_window + 1};
+  tb.lev = Tables::Levels{sm, 2 * T.n_window + 1, 2 * T.n_diff + 1};
+}
 
 __device__ inline void axis_table(double xr, double dk, int M, int X, int n, int cnt, double scale, double2* dst,
                                   int part, int nparts) {
@@ -108,8 +107,20 @@ __device__ inline void axis_table(double xr, double dk, int M, int X, int n, int
   }
 }
 
-// Fill tables for point x with path (levels 2..lmax); block-cooperative.
-__device__ void build_tables(const DevTree& T, const double* x, double q, const int* path, int lmax, Tables& tb) {
+struct Header {
+  int i_orig, slot;
+  double q;
+  double xo[3], xt[3];
+  double dr;
+  int depth_o, depth_t;
+  int path_o[MAXLV], path_t[MAXLV];
+  int Xo[MAXLV][3], Xt[MAXLV][3];  // integer box coordinates along each path
+};
+
+// Tables of one point on its path for levels 2..lmax; block-cooperative.
+// Box-centred phases with the exact decentring root of unity per axis.
+__device__ void build_tables(const DevTree& T, const double* x, double q, const int (*X)[3], int lmax,
+                             const Tables& tb) {
   const int NP = 4;  // pieces per axis
   const int nlev = lmax >= 2 ? lmax - 1 : 0;
   const int ntask = (1 + nlev) * 3 * NP;
@@ -121,146 +132,318 @@ __device__ void build_tables(const DevTree& T, const double* x, double q, const 
       axis_table(x[axis] - 0.5 * T.L, T.delta_k[0], 3, 0, n, cnt, axis == 2 ? q : 1.0, tb.root[axis], part, NP);
     } else {
       int l = slot + 1;
-      int node = path[l];
-      double c[3];
-      int X[3];
-      node_center(T, node, c, X);
+      int Xa = X[l][axis];
       int n = T.n_diff;
       int cnt = axis == 2 ? n + 1 : 2 * n + 1;
-      axis_table(x[axis] - c[axis], T.delta_k[l], 1, X[axis], n, cnt, axis == 2 ? q : 1.0, tb.lev[l][axis], part, NP);
+      axis_table(x[axis] - center_of(T.L, l, Xa), T.delta_k[l], 1, Xa, n, cnt, axis == 2 ? q : 1.0,
+                 tb.lev[l][axis], part, NP);
     }
   }
 }
 
-__device__ inline double2 phase_at(double2* const* ax, int k, int d) {
+template <class A>
+__device__ inline double2 phase_at(const A& ax, int k, int d) {
   int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
   return cmul(ax[2][iz], cmul(ax[1][iy], ax[0][ix]));
 }
 
-struct Header {
-  int i_orig, slot;
-  double q;
-  double xo[3], xt[3];
-  double dr;
-  int depth_o, depth_t;
-  int path_o[MAXLV], path_t[MAXLV];
-};
-
-// resolve the proposal: particle, positions, paths (first warp of the block)
+// Resolve a proposal with the first warp: particle and positions (every lane
+// loads the same words), my_mod wrap, the minimum-image old-new distance
+// (one image per lane, src/energy_shift.cpp:30-41) and both leaf paths
+// (lanes 0-15 the target, 16-31 the origin, one level per lane, from the
+// refinement bitmaps: the reference's locate_particle, src/tree.cpp:204-236).
 __device__ void resolve(const DevTree& T, int i, const double* disp, Header& h) {
-  const int lane = threadIdx.x & 31;
   if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    const int s = T.orig_slot[i];
+    double xo[3], q;
+    if (s < T.n_slots) {
+      xo[0] = T.sx[s];
+      xo[1] = T.sy[s];
+      xo[2] = T.sz[s];
+      q = T.sq[s];
+    } else {
+      const int p = s - T.n_slots;
+      xo[0] = T.px[p];
+      xo[1] = T.py[p];
+      xo[2] = T.pz[p];
+      q = T.pq[p];
+    }
+    const double L = T.L;
+    const double d0 = disp[0], d1 = disp[1], d2 = disp[2];
+    const double xt[3] = {wrap_mod(xo[0] + d0, L), wrap_mod(xo[1] + d1, L), wrap_mod(xo[2] + d2, L)};
+    double dr = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+    if (lane < 27) {
+      const int mx = lane % 3 - 1, my = (lane / 3) % 3 - 1, mz = lane / 9 - 1;
+      const double ax = xt[0] - (xo[0] + mx * L), ay = xt[1] - (xo[1] + my * L), az = xt[2] - (xo[2] + mz * L);
+      dr = fmin(dr, sqrt(ax * ax + ay * ay + az * az));
+    }
+    for (int o = 16; o > 0; o >>= 1) dr = fmin(dr, __shfl_xor_sync(0xffffffffu, dr, o));
+    const int half = lane >> 4, l = lane & 15;
+    const double* p = half == 0 ? xt : xo;
+    const uint32_t g[3] = {grid_coord(p[0], L), grid_coord(p[1], L), grid_coord(p[2], L)};
+    const uint64_t key = morton3(g[0], g[1], g[2]);
+    bool is_leaf = false;
+    int node = -1;
+    if (l < T.max_depth) {
+      const uint64_t cell = l == 0 ? 0 : key >> (3 * (KEY_BITS - l));
+      const bool exists = l <= 1 || bm_get(T.bm[l - 1], cell >> 3);
+      if (exists) {
+        node = l == 0 ? 0
+                      : (l == 1 ? 1 + int(cell) : T.level_start[l] + 8 * bm_rank(T, l - 1, cell >> 3) + int(cell & 7));
+        is_leaf = !(l <= T.maxref && bm_get(T.bm[l], cell));
+      }
+    }
+    const unsigned leaves = (__ballot_sync(0xffffffffu, is_leaf) >> (16 * half)) & 0xffffu;
+    const int leaf_level = __ffs(leaves) - 1;
+    if (l <= leaf_level) {
+      int* path = half == 0 ? h.path_t : h.path_o;
+      int(*X)[3] = half == 0 ? h.Xt : h.Xo;
+      path[l] = node;
+      for (int a = 0; a < 3; ++a) X[l][a] = int(g[a] >> (KEY_BITS - l));
+    }
     if (lane == 0) {
       h.i_orig = i;
-      int s = T.orig_slot[i];
       h.slot = s;
-      double x, y, z, q;
-      if (s < T.n_slots) {
-        x = T.sx[s];
-        y = T.sy[s];
-        z = T.sz[s];
-        q = T.sq[s];
-      } else {
-        int p = s - T.n_slots;
-        x = T.px[p];
-        y = T.py[p];
-        z = T.pz[p];
-        q = T.pq[p];
-      }
       h.q = q;
-      h.xo[0] = x;
-      h.xo[1] = y;
-      h.xo[2] = z;
-      // my_mod wrap and minimum-image distance (src/energy_shift.cpp:30-41)
-      const double L = T.L;
-      h.xt[0] = wrap_mod(x + disp[0], L);
-      h.xt[1] = wrap_mod(y + disp[1], L);
-      h.xt[2] = wrap_mod(z + disp[2], L);
-      double dr = sqrt(disp[0] * disp[0] + disp[1] * disp[1] + disp[2] * disp[2]);
-      for (int mx = -1; mx <= 1; mx++)
-        for (int my = -1; my <= 1; my++)
-          for (int mz = -1; mz <= 1; mz++) {
-            double ax = h.xt[0] - (x + mx * L), ay = h.xt[1] - (y + my * L), az = h.xt[2] - (z + mz * L);
-            dr = fmin(dr, sqrt(ax * ax + ay * ay + az * az));
-          }
+      for (int a = 0; a < 3; ++a) {
+        h.xo[a] = xo[a];
+        h.xt[a] = xt[a];
+      }
       h.dr = dr;
+      h.depth_t = leaf_level + 1;
     }
-    __syncwarp();
-    int dt = warp_path(T, h.xt[0], h.xt[1], h.xt[2], h.path_t);
-    int dO = warp_path(T, h.xo[0], h.xo[1], h.xo[2], h.path_o);
-    if (lane == 0) {
-      h.depth_t = dt;
-      h.depth_o = dO;
-    }
+    if (lane == 16) h.depth_o = leaf_level + 1;
   }
   __syncthreads();
 }
 
 // q * sum_{j in N(leaf)} q_j res(|x - x_j|; bs_leaf), masked r^2 in (eps, b^2)
-// (eval_shift_energy_res_vec + direct_eval, src/energy_shift.cpp:233-302)
-__device__ double residual_sum(const DevTree& T, int leaf, const double* x) {
-  const int l = T.node_level[leaf];
+// (eval_shift_energy_res_vec + direct_eval, src/energy_shift.cpp:233-302).
+// Source metadata is fetched in parallel, then all threads share the pairs.
+__device__ double residual_sum(const DevTree& T, int leaf, int l, const int* Xl, const double* x) {
   const double b = T.boxsize[l];
   const double b2 = b * b;
   const double eps = 2.220446049250313e-16;
-  double ci[3];
-  int Xi[3];
-  node_center(T, leaf, ci, Xi);
-  double acc = 0;
-  // sources: self (0), colleagues (1..27), coarse (28..35)
-  for (int src = threadIdx.x >> 5; src < 36; src += blockDim.x >> 5) {
-    int j;
+  __shared__ int m_beg[36], m_cnt[36], m_pre[37], m_lvl[36];
+  __shared__ unsigned long long m_pfx[36];
+  __shared__ double m_off[36][3];
+  if (threadIdx.x < 36) {
+    const int src = threadIdx.x;
+    int j = -1;
     if (src == 0) j = leaf;
-    else if (src <= 27) {
-      if (src - 1 == 13) continue;
-      j = T.col27[size_t(leaf) * 27 + (src - 1)];
-    } else {
-      j = T.coarse8[size_t(leaf) * 8 + (src - 28)];
+    else if (src <= 27) j = (src - 1 == 13) ? -1 : T.col27[size_t(leaf) * 27 + (src - 1)];
+    else j = T.coarse8[size_t(leaf) * 8 + (src - 28)];
+    int beg = 0, cnt = 0, lj = 0;
+    unsigned long long pj = 0;
+    double off[3] = {0, 0, 0};
+    if (j >= 0) {
+      lj = T.node_level[j];
+      pj = T.node_prefix[j];
+      const int ch = T.node_child0[j];
+      beg = T.node_begin[j];
+      const int end = ch < 0 ? beg + T.leaf_count[j] : T.node_end[j];
+      cnt = end - beg;
+      const double bj = T.boxsize[lj];
+      const int Xj[3] = {int(compact3(pj)), int(compact3(pj >> 1)), int(compact3(pj >> 2))};
+      for (int d = 0; d < 3; ++d)
+        off[d] = -periodic_shift_d(center_of(T.L, l, Xl[d]), center_of(T.L, lj, Xj[d]), T.L, b, bj) * T.L;
     }
-    if (j < 0) continue;
-    double cj[3];
-    int Xj[3];
-    node_center(T, j, cj, Xj);
-    const double bj = T.boxsize[T.node_level[j]];
-    double off[3];
-    for (int d = 0; d < 3; ++d) off[d] = -periodic_shift_d(ci[d], cj[d], T.L, b, bj) * T.L;
-    const bool is_leaf = T.node_child0[j] < 0;
-    const int sb = T.node_begin[j];
-    const int se = is_leaf ? sb + T.leaf_count[j] : T.node_end[j];
-    for (int s = sb + (threadIdx.x & 31); s < se; s += 32) {
-      double dx = x[0] - (T.sx[s] + off[0]), dy = x[1] - (T.sy[s] + off[1]), dz = x[2] - (T.sz[s] + off[2]);
-      double r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 > eps && r2 < b2) acc += T.sq[s] * poly_res(T, sqrt(r2), b);
+    m_beg[src] = beg;
+    m_cnt[src] = j >= 0 ? cnt : -1;
+    m_lvl[src] = lj;
+    m_pfx[src] = pj;
+    for (int d = 0; d < 3; ++d) m_off[src][d] = off[d];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int src = 0; src < 36; ++src) {
+      m_pre[src] = s;
+      s += max(m_cnt[src], 0);
     }
-    // arrivals parked in the overflow pool that belong to j's subtree
-    const int pn = *T.pool_n;
-    const int lj = T.node_level[j];
-    const uint64_t pj = T.node_prefix[j];
-    for (int p = threadIdx.x & 31; p < pn; p += 32) {
-      if (T.p_orig[p] < 0) continue;
-      int pl = T.p_leaf[p];
-      int ll = T.node_level[pl];
-      if (ll < lj || (T.node_prefix[pl] >> (3 * (ll - lj))) != pj) continue;
-      double dx = x[0] - (T.px[p] + off[0]), dy = x[1] - (T.py[p] + off[1]), dz = x[2] - (T.pz[p] + off[2]);
-      double r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 > eps && r2 < b2) acc += T.pq[p] * poly_res(T, sqrt(r2), b);
-    }
+    m_pre[36] = s;
+  }
+  __syncthreads();
+  const int total = m_pre[36];
+  double acc = 0;
+  int src = 0;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    while (e >= m_pre[src + 1]) ++src;
+    const int s = m_beg[src] + (e - m_pre[src]);
+    const double dx = x[0] - (T.sx[s] + m_off[src][0]), dy = x[1] - (T.sy[s] + m_off[src][1]),
+                 dz = x[2] - (T.sz[s] + m_off[src][2]);
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 > eps && r2 < b2) acc += T.sq[s] * poly_res(T, sqrt(r2), b);
+  }
+  // arrivals parked in the overflow pool that belong to a source's subtree
+  const int pn = *T.pool_n;
+  for (int e = threadIdx.x; e < 36 * pn; e += blockDim.x) {
+    const int sj = e / pn, p = e % pn;
+    if (m_cnt[sj] < 0 || T.p_orig[p] < 0) continue;
+    const int pl = T.p_leaf[p];
+    const int ll = T.node_level[pl], lj = m_lvl[sj];
+    if (ll < lj || (T.node_prefix[pl] >> (3 * (ll - lj))) != m_pfx[sj]) continue;
+    const double dx = x[0] - (T.px[p] + m_off[sj][0]), dy = x[1] - (T.py[p] + m_off[sj][1]),
+                 dz = x[2] - (T.pz[p] + m_off[sj][2]);
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 > eps && r2 < b2) acc += T.pq[p] * poly_res(T, sqrt(r2), b);
   }
   return acc;
 }
 
-__device__ inline double block_sum(double v, double* sm) {
+// sums of four values over the block, valid in thread 0
+__device__ inline void block_sum4(double* v, double (*sm)[32]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  for (int c = 0; c < 4; ++c)
+    for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
   __syncthreads();
-  if (lane == 0) sm[warp] = v;
+  if (lane == 0)
+    for (int c = 0; c < 4; ++c) sm[c][warp] = v[c];
   __syncthreads();
-  double s = 0;
   if (threadIdx.x == 0)
-    for (int w = 0; w < nw; ++w) s += sm[w];
+    for (int c = 0; c < 4; ++c) {
+      double s = 0;
+      for (int w = 0; w < nw; ++w) s += sm[c][w];
+      v[c] = s;
+    }
   __syncthreads();
-  return s;
+}
+
+// slot s of a path level: 0 own outgoing, 1 own incoming, 2.. the colleague
+// in direction dir (dir != 13, dx fastest)
+__device__ inline int slot_of_dir(int dir) { return 2 + (dir < 13 ? dir : dir - 1); }
+__device__ inline int dir_of_slot(int s) { return (s - 2) + ((s - 2) >= 13 ? 1 : 0); }
+
+// Receivers of an accepted move (update_shift, src/tree.cpp:484-579): per
+// path level own out, own inc and non-leaf colleagues' inc. A vector that
+// both paths touch becomes one receiver carrying both contributions, so the
+// update needs a single launch without write races. Receivers are matched by
+// box coordinates (known from the header), the records go to T.recv and the
+// count is returned to every thread. Block-cooperative.
+__device__ int build_receivers(const DevTree& T, const Header& h) {
+  constexpr int PER = 28 * MAXLV;
+  __shared__ int ckey[2 * PER];  // receiving node (-1 none)
+  __shared__ signed char cfl[2 * PER][3];
+  __shared__ short cmatch[2 * PER];
+  __shared__ int wsum[32];
+  const int levels = max(T.pw_hi - 1, 0);
+  const int per = 28 * levels;
+  const int ncand = 2 * per;
+  const int ut = min(h.depth_t - 1, T.pw_hi), uo = min(h.depth_o - 1, T.pw_hi);
+  for (int c = threadIdx.x; c < ncand; c += blockDim.x) {
+    const int p = c / per, r = c % per;
+    const int l = 2 + r / 28, s = r % 28;
+    int recv = -1;
+    signed char f[3] = {0, 0, 0};
+    if (l <= (p == 0 ? ut : uo)) {
+      const int node = p == 0 ? h.path_t[l] : h.path_o[l];
+      recv = node;
+      if (s >= 2) {
+        const int dir = dir_of_slot(s);
+        recv = T.col27[size_t(node) * 27 + dir];
+        if (recv >= 0 && T.node_child0[recv] < 0) recv = -1;
+        if (recv >= 0) {
+          // source-centric image flag: periodic_shift(c_source, c_receiver)
+          const int* X = p == 0 ? h.Xt[l] : h.Xo[l];
+          const int dv[3] = {dir % 3 - 1, (dir / 3) % 3 - 1, dir / 9 - 1};
+          for (int q = 0; q < 3; ++q) {
+            const int v = X[q] + dv[q];
+            f[q] = v < 0 ? 1 : (v >= (1 << l) ? -1 : 0);
+          }
+        }
+      }
+    }
+    ckey[c] = recv;
+    cfl[c][0] = f[0];
+    cfl[c][1] = f[1];
+    cfl[c][2] = f[2];
+    cmatch[c] = -1;
+  }
+  __syncthreads();
+  // an origin receiver equals a target receiver when it is the same vector;
+  // its slot among the target's follows from the box coordinates
+  for (int c = per + threadIdx.x; c < ncand; c += blockDim.x) {
+    const int recv = ckey[c];
+    if (recv < 0) continue;
+    const int r = c - per, l = 2 + r / 28, s = r % 28;
+    if (l > ut) continue;
+    const int e = 1 << l;
+    int ts;
+    if (s == 0) {
+      ts = h.path_t[l] == recv ? 0 : -1;
+    } else {
+      // receiver coordinates relative to the target's box at this level
+      const int dir_o = s == 1 ? 13 : dir_of_slot(s);
+      const int dvo[3] = {dir_o % 3 - 1, (dir_o / 3) % 3 - 1, dir_o / 9 - 1};
+      int dir = 0, mul = 1;
+      bool ok = true;
+      for (int q = 0; q < 3; ++q) {
+        int dq = ((h.Xo[l][q] + dvo[q] + e) & (e - 1)) - h.Xt[l][q];
+        if (dq == e - 1) dq = -1;
+        if (dq == 1 - e) dq = 1;
+        ok = ok && dq >= -1 && dq <= 1;
+        dir += (dq + 1) * mul;
+        mul *= 3;
+      }
+      ts = !ok ? -1 : (dir == 13 ? 1 : slot_of_dir(dir));
+    }
+    if (ts >= 0) {
+      const int t = (l - 2) * 28 + ts;
+      if (ckey[t] == recv) {
+        cmatch[c] = short(t);
+        cmatch[t] = short(c);
+      }
+    }
+  }
+  __syncthreads();
+  // compact: target receivers in slot order, then unmatched origin receivers
+  const int per_thread = (ncand + blockDim.x - 1) / blockDim.x;
+  const int c0 = threadIdx.x * per_thread;
+  int cnt = 0;
+  for (int c = c0; c < min(c0 + per_thread, ncand); ++c) cnt += ckey[c] >= 0 && (c < per || cmatch[c] < 0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+      int v = wsum[w];
+      wsum[w] = s;
+      s += v;
+    }
+    wsum[31] = s;
+  }
+  __syncthreads();
+  int pos = wsum[warp] + x - cnt;
+  const int base = T.level_start[T.pw_lo];
+  for (int c = c0; c < min(c0 + per_thread, ncand); ++c) {
+    if (!(ckey[c] >= 0 && (c < per || cmatch[c] < 0))) continue;
+    const int r = c % per;
+    Receiver R;
+    R.off = ckey[c] - base;
+    R.is_out = (r % 28) == 0;
+    R.level = static_cast<signed char>(2 + r / 28);
+    const bool is_t = c < per;
+    const int m = cmatch[c];
+    R.has_t = is_t;
+    R.has_o = !is_t || m >= 0;
+    for (int q = 0; q < 3; ++q) {
+      R.ft[q] = is_t ? cfl[c][q] : 0;
+      R.fo[q] = is_t ? (m >= 0 ? cfl[m][q] : 0) : cfl[c][q];
+    }
+    R.pad[0] = R.pad[1] = 0;
+    T.recv[pos++] = R;
+  }
+  const int total = wsum[31];
+  __syncthreads();
+  return total;
 }
 
 struct ShiftArgs {
@@ -272,49 +455,65 @@ struct ShiftArgs {
   int mode;  // 0: evaluate only, 1: Metropolis
   double* dE_out;
   int* acc_out;
-  double c_window;  // dk_0^3 / (2 pi)^3
+  double c_window;            // dk_0^3 / (2 pi)^3
   double c_level[MAXLV + 2];  // dk_l^3 / (2 pi)^3 * dscale_l
   double* partials;
   unsigned int* counter;
   Proposal* prop;
+  double2* ptab;          // phase tables published for k_update
+  long ptab_per;          // complex entries per path
+  const MoveCursor* cur;  // non-null: proposals come from the cursor (captured graphs)
 };
-
-__device__ inline void alloc_tables(double2* sm, const DevTree& T, Tables& tb, int lmax) {
-  double2* p = sm;
-  for (int a = 0; a < 3; ++a) {
-    tb.root[a] = p;
-    p += 2 * T.n_window + 1;
-  }
-  for (int l = 2; l <= lmax; ++l)
-    for (int a = 0; a < 3; ++a) {
-      tb.lev[l][a] = p;
-      p += 2 * T.n_diff + 1;
-    }
-}
 
 // Grid: blocks [0, G-2) do the plane-wave sums; block G-2 the target
 // residual, block G-1 the origin residual. The last block to finish reduces.
 __global__ void __launch_bounds__(SH_T) k_shift(DevTree T, ShiftArgs a) {
   extern __shared__ double2 sm2[];
   __shared__ Header h;
-  __shared__ double red[32];
+  __shared__ double red[4][32];
   __shared__ bool is_last;
+  if (a.cur) {
+    const MoveCursor c = *a.cur;
+    a.idx = c.idx;
+    a.disp = c.disp;
+    a.u = c.u;
+    a.dE_out = c.dE;
+    a.acc_out = c.acc;
+    a.mode = c.mode;
+    a.beta = c.beta;
+    a.move += c.off;
+  }
   const int move = a.move;
   resolve(T, a.idx[move], a.disp + 3 * move, h);
   const int G = gridDim.x;
   const int Gpw = G - 2;
-  double acc_w = 0, acc_d = 0, res_t = 0, res_o = 0;
+  double acc[4] = {0, 0, 0, 0};  // window, difference, residual target, residual origin
   if (blockIdx.x < Gpw) {
-    // non-leaf path levels: 2 .. depth-2
+    // dE needs the non-leaf path levels 2 .. depth-2; an accept-and-update
+    // needs 2 .. min(depth-1, pw_hi): build the superset
     const int lo_max = h.depth_o - 2, lt_max = h.depth_t - 2;
+    const int uo = min(h.depth_o - 1, T.pw_hi), ut = min(h.depth_t - 1, T.pw_hi);
+    const int per = 3 * (2 * T.n_window + 1) + max(max(uo, ut) - 1, 0) * 3 * (2 * T.n_diff + 1);
     Tables to, oo;
-    const int lmax = max(lo_max, lt_max);
-    const int per = 3 * (2 * T.n_window + 1) + (lmax >= 2 ? (lmax - 1) : 0) * 3 * (2 * T.n_diff + 1);
-    alloc_tables(sm2, T, oo, lmax);
-    alloc_tables(sm2 + per, T, to, lmax);
-    build_tables(T, h.xo, h.q, h.path_o, lo_max, oo);
-    build_tables(T, h.xt, h.q, h.path_t, lt_max, to);
+    alloc_tables(sm2, T, oo);
+    alloc_tables(sm2 + per, T, to);
+    build_tables(T, h.xo, h.q, h.Xo, uo, oo);
+    build_tables(T, h.xt, h.q, h.Xt, ut, to);
     __syncthreads();
+    if (blockIdx.x == 0) {
+      // publish the tables for k_update
+      for (int p = 0; p < 2; ++p) {
+        Tables g;
+        alloc_tables(a.ptab + size_t(p) * a.ptab_per, T, g);
+        const Tables& s = p == 0 ? oo : to;
+        const int up = p == 0 ? uo : ut;
+        for (int ax = 0; ax < 3; ++ax)
+          for (int e = threadIdx.x; e < T.dw; e += blockDim.x) g.root[ax][e] = s.root[ax][e];
+        for (int l = 2; l <= up; ++l)
+          for (int ax = 0; ax < 3; ++ax)
+            for (int e = threadIdx.x; e < T.dd; e += blockDim.x) g.lev[l][ax][e] = s.lev[l][ax][e];
+      }
+    }
     const int stride = Gpw * blockDim.x;
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
     // window (src/energy_shift.cpp:72-90)
@@ -322,63 +521,56 @@ __global__ void __launch_bounds__(SH_T) k_shift(DevTree T, ShiftArgs a) {
       double2 t = phase_at(to.root, k, T.dw), o = phase_at(oo.root, k, T.dw);
       double2 g = T.out_root[k];
       double ar = t.x - o.x, ai = t.y - o.y, br = g.x - o.x, bi = g.y - o.y;
-      acc_w += (ar * br + ai * bi) * T.W[k];
+      acc[0] += (ar * br + ai * bi) * T.W[k];
     }
-    // difference (src/energy_shift.cpp:92-140)
+    // difference (src/energy_shift.cpp:92-140), all path levels per mode
     const int base = T.level_start[T.pw_lo];
-    for (int l = 2; l <= lo_max; ++l) {
-      const double2* inc = T.inc + size_t(h.path_o[l] - base) * T.H;
+    const int d = T.dd;
+    for (int k = t0; k < T.H; k += stride) {
+      const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
       double s = 0;
-      for (int k = t0; k < T.H; k += stride) {
-        double2 o = phase_at(oo.lev[l], k, T.dd);
-        double2 c = inc[k];
-        s += (o.x * c.x - o.y * c.y - (o.x * o.x + o.y * o.y)) * T.D2[k];
+      for (int l = 2; l <= lo_max; ++l) {
+        double2 o = cmul(oo.lev[l][2][iz], cmul(oo.lev[l][1][iy], oo.lev[l][0][ix]));
+        double2 c = T.inc[size_t(h.path_o[l] - base) * T.H + k];
+        s -= (o.x * c.x - o.y * c.y - (o.x * o.x + o.y * o.y)) * a.c_level[l];
       }
-      acc_d -= s * a.c_level[l];
-    }
-    for (int l = 2; l <= lt_max; ++l) {
-      const double2* inc = T.inc + size_t(h.path_t[l] - base) * T.H;
-      double s = 0;
-      for (int k = t0; k < T.H; k += stride) {
-        double2 t = phase_at(to.lev[l], k, T.dd);
-        double2 c = inc[k];
-        s += (t.x * c.x - t.y * c.y) * T.D2[k];
+      for (int l = 2; l <= lt_max; ++l) {
+        double2 t = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
+        double2 c = T.inc[size_t(h.path_t[l] - base) * T.H + k];
+        s += (t.x * c.x - t.y * c.y) * a.c_level[l];
       }
-      acc_d += s * a.c_level[l];
+      acc[1] += s * T.D2[k];
     }
   } else if (blockIdx.x == Gpw) {
-    res_t = residual_sum(T, h.path_t[h.depth_t - 1], h.xt) * h.q;
+    const int lt = h.depth_t - 1;
+    acc[2] = residual_sum(T, h.path_t[lt], lt, h.Xt[lt], h.xt) * h.q;
   } else {
-    res_o = residual_sum(T, h.path_o[h.depth_o - 1], h.xo) * h.q;
+    const int lo = h.depth_o - 1;
+    acc[3] = residual_sum(T, h.path_o[lo], lo, h.Xo[lo], h.xo) * h.q;
   }
-  double sw = block_sum(acc_w, red), sd = block_sum(acc_d, red);
-  double st = block_sum(res_t, red), so = block_sum(res_o, red);
+  block_sum4(acc, red);
   if (threadIdx.x == 0) {
     double* pp = a.partials + 4 * size_t(blockIdx.x);
-    pp[0] = sw;
-    pp[1] = sd;
-    pp[2] = st;
-    pp[3] = so;
+    for (int c = 0; c < 4; ++c) pp[c] = acc[c];
     __threadfence();
     unsigned prev = atomicAdd(a.counter, 1u);
     is_last = (prev == unsigned(G - 1));
   }
   __syncthreads();
-  if (is_last && threadIdx.x == 0) {
-    __threadfence();
-    double w = 0, d = 0, rt = 0, ro = 0;
-    for (int b = 0; b < G; ++b) {
-      const double* pp = a.partials + 4 * size_t(b);
-      w += __ldcg(pp);
-      d += __ldcg(pp + 1);
-      rt += __ldcg(pp + 2);
-      ro += __ldcg(pp + 3);
-    }
-    double dEw = 2.0 * w * 0.5 * a.c_window;
-    double r = h.dr;
+  if (!is_last) return;
+  __threadfence();
+  // fixed-order reduction of the block partials (deterministic)
+  double tot[4] = {0, 0, 0, 0};
+  for (int b = threadIdx.x; b < G; b += blockDim.x)
+    for (int c = 0; c < 4; ++c) tot[c] += __ldcg(a.partials + 4 * size_t(b) + c);
+  block_sum4(tot, red);
+  const int nrecv = build_receivers(T, h);
+  if (threadIdx.x == 0) {
+    const double dEw = tot[0] * a.c_window;  // 2 * sum * dk0^3 / (2 (2 pi)^3)
+    const double d = tot[1], rt = tot[2], ro = tot[3];
     double self = 0;
-    if (r != 0) self = poly_res(T, r, T.boxsize[2]) * h.q * h.q;
-    double dE = dEw + d + rt - ro - self;
+    if (h.dr != 0) self = poly_res(T, h.dr, T.boxsize[2]) * h.q * h.q;
+    const double dE = dEw + d + rt - ro - self;
     Proposal* P = a.prop;
     P->i_orig = h.i_orig;
     P->slot = h.slot;
@@ -399,135 +591,110 @@ __global__ void __launch_bounds__(SH_T) k_shift(DevTree T, ShiftArgs a) {
     P->parts[2] = rt;
     P->parts[3] = ro;
     P->parts[4] = self;
-    int acc = 0;
+    int accd = 0;
     if (a.mode == 1) {
-      double u = a.u[move];
-      acc = u < exp(-a.beta * dE) ? 1 : 0;
-      if (a.acc_out) a.acc_out[move] = acc;
+      const double u = a.u[move];
+      accd = u < exp(-a.beta * dE) ? 1 : 0;
+      if (a.acc_out) a.acc_out[move] = accd;
     }
     if (a.dE_out) a.dE_out[move] = dE;
-    P->accepted = acc;
+    P->accepted = accd;
     P->valid = 1;
+    P->n_recv = nrecv;
     *a.counter = 0u;
   }
 }
 
 // ---------------------------------------------------------------------------
-// update_shift (src/tree.cpp:447-597) for one path: sign +1 target, -1 origin
-__global__ void __launch_bounds__(SH_T) k_update(DevTree T, int which, double c_unused) {
-  extern __shared__ double2 sm2[];
-  __shared__ int rnode[MAXLV * 28];
-  __shared__ signed char rflag[MAXLV * 28][4];  // is_out, px, py, pz
-  __shared__ int rlevel[MAXLV * 28];
-  __shared__ int nrecv;
-  __shared__ Proposal P;
-  if (threadIdx.x == 0) P = *T.prop;
+// update_shift (src/tree.cpp:447-597) in one launch. Each thread owns one
+// mode k (grid x) and walks a range of receivers (grid y): out += t - o, or
+// inc += conj(t s_t) - conj(o s_o) with the periodic image phases s; the
+// y == 0 blocks also update the root expansion (out += t; out -= o) and
+// block (0, 0) commits the particle membership.
+constexpr int UPD_T = 128;
+constexpr int UPD_UNROLL = 8;
+
+__device__ void commit_move(const DevTree& T);
+
+__device__ inline double2 image_phase(double2 p, const signed char* f, int ix, int iy, int iz, int n, int two_l) {
+  if (f[0] | f[1] | f[2]) {
+    const int sg = ((ix - n) * f[0] + (iy - n) * f[1] + (iz - n) * f[2]) * two_l;
+    p = cmul(p, root6(-2 * (sg % 3)));
+  }
+  return p;
+}
+
+__global__ void __launch_bounds__(UPD_T) k_update(DevTree T, const double2* __restrict__ ptab, long ptab_per) {
+  __shared__ Receiver rs[MAX_RECV];
+  __shared__ int s_acc, s_nr;
+  if (threadIdx.x == 0) {
+    s_acc = T.prop->accepted;
+    s_nr = T.prop->n_recv;
+  }
   __syncthreads();
-  if (!P.accepted) return;
-  const bool tgt = which == 0;
-  const double sign = tgt ? 1.0 : -1.0;
-  const int depth = tgt ? P.depth_t : P.depth_o;
-  const int* path = tgt ? P.path_t : P.path_o;
-  const double* x = tgt ? P.xt : P.xo;
-  const int lmax = min(depth - 1, T.pw_hi);  // path levels 2..leaf level carrying expansions
-  // receivers per level: own out, own inc, non-leaf colleagues' inc
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    if (lane == 0) nrecv = 0;
-    __syncwarp();
-    for (int l = 2; l <= lmax; ++l) {
-      const int node = path[l];
-      uint64_t p = T.node_prefix[node];
-      int X[3] = {int(compact3(p)), int(compact3(p >> 1)), int(compact3(p >> 2))};
-      int j = -1;
-      bool ok = false;
-      if (lane < 27 && lane != 13) {
-        j = T.col27[size_t(node) * 27 + lane];
-        ok = j >= 0 && T.node_child0[j] >= 0;
-      }
-      unsigned m = __ballot_sync(0xffffffffu, ok);
-      int base = nrecv;
-      if (ok) {
-        int pos = base + 2 + __popc(m & ((1u << lane) - 1u));
-        rnode[pos] = j;
-        rlevel[pos] = l;
-        rflag[pos][0] = 0;
-        int dv[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
-        for (int d = 0; d < 3; ++d) {
-          // source-centric image flag: periodic_shift(c_source, c_receiver)
-          int v = X[d] + dv[d];
-          rflag[pos][1 + d] = v < 0 ? 1 : (v >= (1 << l) ? -1 : 0);
+  if (!s_acc) return;
+  const int nr = s_nr;
+  const int r0 = int((long(blockIdx.y) * nr) / gridDim.y), r1 = int((long(blockIdx.y + 1) * nr) / gridDim.y);
+  for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) rs[r - r0] = T.recv[r];
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    atomicAdd(&T.work[0], 1ull);
+    atomicAdd(&T.work[1], 32ull * ((unsigned long long)T.Hw + (unsigned long long)nr * T.H));
+    commit_move(T);
+  }
+  __syncthreads();
+  Tables tt, to;
+  alloc_tables(const_cast<double2*>(ptab) + ptab_per, T, tt);
+  alloc_tables(const_cast<double2*>(ptab), T, to);
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (blockIdx.y == 0 && k < T.Hw) {
+    double2 t = phase_at(tt.root, k, T.dw), o = phase_at(to.root, k, T.dw);
+    double2 g = T.out_root[k];
+    g = cadd(g, t);
+    g = csub(g, o);
+    T.out_root[k] = g;
+  }
+  if (k >= T.H) return;
+  const int n = T.n_diff, d = T.dd;
+  const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
+  int r = 0;
+  const int nloc = r1 - r0;
+  while (r < nloc) {
+    // a run of receivers on one level shares the two single-particle phases
+    const int l = rs[r].level;
+    int re = r + 1;
+    while (re < nloc && rs[re].level == l) ++re;
+    const double2 pt = cmul(tt.lev[l][2][iz], cmul(tt.lev[l][1][iy], tt.lev[l][0][ix]));
+    const double2 po = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
+    const int two_l = (l & 1) ? 2 : 1;
+    for (; r < re; r += UPD_UNROLL) {
+      double2 v[UPD_UNROLL];
+      size_t off[UPD_UNROLL];
+#pragma unroll
+      for (int u = 0; u < UPD_UNROLL; ++u) {
+        if (r + u < re) {
+          const Receiver& R = rs[r + u];
+          off[u] = size_t(R.off) * T.H + k;
+          v[u] = R.is_out ? T.out[off[u]] : T.inc[off[u]];
         }
       }
-      if (lane < 2) {
-        rnode[base + lane] = node;
-        rlevel[base + lane] = l;
-        rflag[base + lane][0] = lane == 0 ? 1 : 0;
-        rflag[base + lane][1] = rflag[base + lane][2] = rflag[base + lane][3] = 0;
+#pragma unroll
+      for (int u = 0; u < UPD_UNROLL; ++u) {
+        if (r + u < re) {
+          const Receiver& R = rs[r + u];
+          double2 del = make_double2(0.0, 0.0);
+          if (R.has_t) del = image_phase(pt, R.ft, ix, iy, iz, n, two_l);
+          if (R.has_o) del = csub(del, image_phase(po, R.fo, ix, iy, iz, n, two_l));
+          if (R.is_out) T.out[off[u]] = cadd(v[u], del);
+          else T.inc[off[u]] = make_double2(v[u].x + del.x, v[u].y - del.y);
+        }
       }
-      __syncwarp();
-      if (lane == 0) nrecv = base + 2 + __popc(m);
-      __syncwarp();
     }
-  }
-  __syncthreads();
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    // algorithmic update traffic: one read and one write of 16 B per complex
-    unsigned long long b = 32ull * (unsigned long long)nrecv * (unsigned long long)T.H;
-    if (tgt) {
-      b += 32ull * (unsigned long long)T.Hw;
-      atomicAdd(&T.work[0], 1ull);
-    }
-    atomicAdd(&T.work[1], b);
-  }
-  // tables: this path's levels, plus both roots (window) for the target pass
-  Tables tb, tb_o;
-  const int per = 3 * (2 * T.n_window + 1) + (lmax >= 2 ? (lmax - 1) : 0) * 3 * (2 * T.n_diff + 1);
-  alloc_tables(sm2, T, tb, lmax);
-  alloc_tables(sm2 + per, T, tb_o, 0);
-  build_tables(T, x, P.q, path, lmax, tb);
-  if (tgt) build_tables(T, P.xo, P.q, P.path_o, 0, tb_o);
-  __syncthreads();
-  const int stride = gridDim.x * blockDim.x;
-  const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
-  if (tgt) {
-    // root: out += t; out -= o (src/tree.cpp:479-480)
-    for (int k = t0; k < T.Hw; k += stride) {
-      double2 t = phase_at(tb.root, k, T.dw), o = phase_at(tb_o.root, k, T.dw);
-      double2 g = T.out_root[k];
-      g = cadd(g, t);
-      g = csub(g, o);
-      T.out_root[k] = g;
-    }
-  }
-  const int base = T.level_start[T.pw_lo];
-  const int n = T.n_diff, d = T.dd;
-  const long total = long(nrecv) * T.H;
-  for (long e = t0; e < total; e += stride) {
-    const int r = int(e / T.H), k = int(e % T.H);
-    const int l = rlevel[r];
-    double2 p = phase_at(tb.lev[l], k, d);
-    const int is_out = rflag[r][0];
-    const size_t off = size_t(rnode[r] - base) * T.H + k;
-    if (is_out) {
-      double2 v = T.out[off];
-      T.out[off] = make_double2(v.x + sign * p.x, v.y + sign * p.y);
-    } else {
-      const int px = rflag[r][1], py = rflag[r][2], pz = rflag[r][3];
-      if (px | py | pz) {
-        int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
-        int sgn = ((ix - n) * px + (iy - n) * py + (iz - n) * pz) * ((l & 1) ? 2 : 1);
-        p = cmul(p, root6(-2 * (sgn % 3)));
-      }
-      double2 v = T.inc[off];
-      T.inc[off] = make_double2(v.x + sign * p.x, v.y - sign * p.y);
-    }
+    r = re;
   }
 }
 
-// particle membership and position (exact on every level)
-__global__ void k_commit(DevTree T) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// particle membership and position (exact on every level); one thread
+__device__ void commit_move(const DevTree& T) {
   const Proposal P = *T.prop;
   if (!P.accepted) return;
   const int leafA = P.path_o[P.depth_o - 1];
@@ -604,6 +771,7 @@ __global__ void k_commit(DevTree T) {
   for (int l = 0; l < P.depth_t; ++l) T.node_count[P.path_t[l]] += 1;
 }
 
+
 size_t tables_smem(const DevTree& T, int lmax, int copies) {
   size_t per = 3 * size_t(2 * T.n_window + 1) + size_t(std::max(lmax - 1, 0)) * 3 * (2 * T.n_diff + 1);
   return per * copies * sizeof(double2);
@@ -630,43 +798,92 @@ void DmkTree::launch_shift(const int* d_idx, const double* d_disp, const double*
   a.partials = D.partials;
   a.counter = D.counter;
   a.prop = D.prop;
+  ensure_move_resources();
+  a.cur = use_cursor_ ? d_cursor_ : nullptr;
+  a.ptab = ptab_;
+  a.ptab_per = ptab_per_;
   size_t smem = tables_smem(D, D.max_depth, 2);
-  if (shift_grid_ == 0) {
-    int dev = 0, sms = 148;
-    PDMK_CUDA(cudaGetDevice(&dev));
-    PDMK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    shift_grid_ = 2 + sms;
-    static size_t smem_set = 0;  // the attribute is per function, shared by all trees
-    if (smem > smem_set) {
-      PDMK_CUDA(cudaFuncSetAttribute(k_shift, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-      PDMK_CUDA(cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-      smem_set = smem;
-    }
-  }
   time_begin(0);
   k_shift<<<unsigned(shift_grid_), SH_T, smem, st_>>>(D, a);
   PDMK_LAUNCH_CHECK();
   time_end(0);
 }
 
+void DmkTree::launch_shift_cursor(int move) {
+  // proposals, outputs, mode and beta come from *d_cursor_ at run time
+  use_cursor_ = true;
+  launch_shift(nullptr, nullptr, nullptr, 0.0, move, 1, nullptr, nullptr);
+  use_cursor_ = false;
+}
+
+// Per-tree resources of the move kernels, set up before any graph capture
+// (no allocation or attribute change may happen inside a capture).
+void DmkTree::ensure_move_resources() {
+  DevTree& D = dev_;
+  if (!ptab_) {
+    ptab_per_ = 3L * (2 * D.n_window + 1) + long(MAX_LEVELS + 1) * 3 * (2 * D.n_diff + 1);
+    ptab_ = static_cast<double2*>(alloc(sizeof(double2) * 2 * size_t(ptab_per_)));
+    d_cursor_ = static_cast<MoveCursor*>(alloc(sizeof(MoveCursor)));
+  }
+  if (shift_grid_ == 0) {
+    int dev = 0, sms = 148;
+    PDMK_CUDA(cudaGetDevice(&dev));
+    PDMK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    shift_grid_ = 2 + sms;
+    const size_t smem = tables_smem(D, D.max_depth, 2);
+    static size_t smem_set = 0;  // the attribute is per function, shared by all trees
+    if (smem > smem_set) {
+      PDMK_CUDA(cudaFuncSetAttribute(k_shift, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      smem_set = smem;
+    }
+  }
+}
+
+// Capture kGraphMoves sequential moves (shift, update, commit) into one
+// executable graph; with timed != 0 external event records bracket each
+// update so its duration can be read after the graph ran.
+void DmkTree::build_mc_graph(int timed) {
+  ensure_move_resources();
+  if (timed && graph_ev_.empty()) {
+    graph_ev_.resize(2 * kGraphMoves);
+    for (auto& e : graph_ev_) PDMK_CUDA(cudaEventCreate(&e));
+  }
+  cudaGraph_t g;
+  capturing_ = true;
+  PDMK_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+  try {
+    for (int b = 0; b < kGraphMoves; ++b) {
+      launch_shift_cursor(b);
+      if (timed) PDMK_CUDA(cudaEventRecordWithFlags(graph_ev_[2 * b], st_, cudaEventRecordExternal));
+      launch_update();
+      if (timed) PDMK_CUDA(cudaEventRecordWithFlags(graph_ev_[2 * b + 1], st_, cudaEventRecordExternal));
+    }
+  } catch (...) {
+    capturing_ = false;
+    cudaStreamEndCapture(st_, &g);
+    throw;
+  }
+  PDMK_CUDA(cudaStreamEndCapture(st_, &g));
+  capturing_ = false;
+  PDMK_CUDA(cudaGraphInstantiate(&mc_graph_[timed], g, 0));
+  PDMK_CUDA(cudaGraphDestroy(g));
+}
+
 void DmkTree::launch_update() {
   DevTree& D = dev_;
-  size_t smem = tables_smem(D, D.max_depth, 2);
-  if (update_grid_ == 0) update_grid_ = 2 * 148;
+  const int levels = std::max(D.pw_hi - 1, 0);
+  // rows: root, up to 2 x 28 receivers per expansion level, commit
+  // x: one mode per thread; y: receiver ranges, enough for ~16 warps per SM
+  const int gx = (std::max(D.H, D.Hw) + UPD_T - 1) / UPD_T;
+  const int gy = std::max(1, std::min(8, (16 * (shift_grid_ - 2) * 32 / UPD_T + gx - 1) / std::max(gx, 1)));
+  (void)levels;
+  const dim3 grid{unsigned(gx), unsigned(gy), 1u};
   time_begin(1);
-  k_update<<<unsigned(update_grid_), SH_T, smem, st_>>>(D, 0, 0.0);
-  PDMK_LAUNCH_CHECK();
-  k_update<<<unsigned(update_grid_), SH_T, smem, st_>>>(D, 1, 0.0);
+  k_update<<<grid, UPD_T, 0, st_>>>(D, ptab_, ptab_per_);
   PDMK_LAUNCH_CHECK();
   time_end(1);
 }
 
-void DmkTree::launch_commit() {
-  time_begin(2);
-  k_commit<<<1, 32, 0, st_>>>(dev_);
-  PDMK_LAUNCH_CHECK();
-  time_end(2);
-}
 
 cudaEvent_t DmkTree::take_event() {
   if (!ev_pool_.empty()) {
@@ -680,13 +897,13 @@ cudaEvent_t DmkTree::take_event() {
 }
 
 void DmkTree::time_begin(int cls) {
-  if (!timing_) return;
+  if (!timing_ || capturing_) return;
   ev_cur_[cls] = take_event();
   PDMK_CUDA(cudaEventRecord(ev_cur_[cls], st_));
 }
 
 void DmkTree::time_end(int cls) {
-  if (!timing_ || !ev_cur_[cls]) return;
+  if (!timing_ || capturing_ || !ev_cur_[cls]) return;
   cudaEvent_t e = take_event();
   PDMK_CUDA(cudaEventRecord(e, st_));
   ev_open_.push_back({cls, {ev_cur_[cls], e}});
@@ -751,7 +968,6 @@ void DmkTree::update_shift(long i, double dx, double dy, double dz) {
   int one = 1;
   PDMK_CUDA(cudaMemcpyAsync(&dev_.prop->accepted, &one, sizeof(int), cudaMemcpyHostToDevice, st_));
   launch_update();
-  launch_commit();
   PDMK_CUDA(cudaStreamSynchronize(st_));
   last_valid_ = false;
   diff_cached_ = false;
@@ -759,10 +975,30 @@ void DmkTree::update_shift(long i, double dx, double dy, double dz) {
 
 void DmkTree::mc_run_device(int n_moves, const int* d_idx, const double* d_disp, const double* d_u, double beta,
                             double* d_dE, int* d_acc) {
-  for (int m = 0; m < n_moves; ++m) {
+  ensure_move_resources();
+  const int timed = timing_ ? 1 : 0;
+  int m = 0;
+  // whole batches run as one captured graph each
+  while (n_moves - m >= kGraphMoves) {
+    if (!mc_graph_[timed]) build_mc_graph(timed);
+    MoveCursor c{d_idx, d_disp, d_u, d_dE, d_acc, m, 1, beta};
+    PDMK_CUDA(cudaMemcpyAsync(d_cursor_, &c, sizeof(c), cudaMemcpyHostToDevice, st_));
+    PDMK_CUDA(cudaGraphLaunch(mc_graph_[timed], st_));
+    if (timed) {
+      // the events are reused by the next launch: read them now
+      PDMK_CUDA(cudaStreamSynchronize(st_));
+      for (int b = 0; b < kGraphMoves; ++b) {
+        float ms = 0;
+        PDMK_CUDA(cudaEventElapsedTime(&ms, graph_ev_[2 * b], graph_ev_[2 * b + 1]));
+        t_ms_[1] += ms;
+        t_cnt_[1] += 1;
+      }
+    }
+    m += kGraphMoves;
+  }
+  for (; m < n_moves; ++m) {
     launch_shift(d_idx, d_disp, d_u, beta, m, 1, d_dE, d_acc);
     launch_update();
-    launch_commit();
   }
   last_valid_ = false;
   diff_cached_ = false;

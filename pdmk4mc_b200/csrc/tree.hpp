@@ -32,6 +32,33 @@ struct Proposal {
   double parts[5];  // window, difference, residual(target), residual(origin), self
   int accepted;
   int valid;
+  int n_recv;  // expansion vectors an accepted move updates (records in DevTree::recv)
+};
+
+// One expansion vector touched by an accepted move, with the contributions of
+// the target (+) and origin (-) single-particle expansions and the periodic
+// image flags of each source box as seen from the receiving box.
+struct Receiver {
+  int off;              // (node - first expansion node), selects out/inc row
+  signed char is_out;   // 1: outgoing (no conjugate, no shift), 0: incoming
+  signed char level;
+  signed char has_t, has_o;
+  signed char ft[3], fo[3];
+  signed char pad[2];
+};
+constexpr int MAX_RECV = 2 * 28 * MAX_LEVELS;
+
+// Where the captured Metropolis graph reads its proposals: set before each
+// launch of the graph, so one instantiated graph serves every batch.
+struct MoveCursor {
+  const int* idx;
+  const double* disp;
+  const double* u;
+  double* dE;
+  int* acc;
+  int off;
+  int mode;
+  double beta;
 };
 
 // Everything the kernels need, by value (all pointers are device pointers).
@@ -86,6 +113,7 @@ struct DevTree {
   double* partials;
   unsigned int* counter;
   Proposal* prop;
+  Receiver* recv;  // [MAX_RECV]
   int* err;  // device error word (nonzero: pool overflow etc.)
   unsigned long long* work;  // [0] accepted moves, [1] update bytes (read + write)
 };
@@ -150,8 +178,7 @@ class DmkTree {
   size_t partials_needed() const;
   void launch_shift(const int* d_idx, const double* d_disp, const double* d_u, double beta, int move, int mode,
                     double* d_dE, int* d_acc);
-  void launch_update();
-  void launch_commit();
+  void launch_update();  // accept-and-update and membership commit, one launch
   void ensure_packed();
   void prepare_box_lists();
   void run_incoming(bool write_inc);
@@ -210,7 +237,20 @@ class DmkTree {
   cudaEvent_t ev_cur_[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t take_event();
   int shift_grid_ = 0;
-  int update_grid_ = 0;
+  // captured Metropolis batches (plain, and with per-update timing events)
+  static constexpr int kGraphMoves = 128;
+  cudaGraphExec_t mc_graph_[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> graph_ev_;  // [2 * kGraphMoves] start/end of each update
+  MoveCursor* d_cursor_ = nullptr;
+  bool capturing_ = false;
+  bool use_cursor_ = false;
+  void ensure_move_resources();
+  void build_mc_graph(int timed);
+  void launch_shift_cursor(int move);
+  cudaStream_t aux_ = nullptr;  // second stream for the root plane-wave pass
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+  double2* ptab_ = nullptr;  // phase tables of the last proposal, both paths
+  long ptab_per_ = 0;
   // host-side copy of the last proposal arguments (for update_shift)
   long last_i_ = -1;
   double last_d_[3] = {0, 0, 0};

@@ -143,7 +143,11 @@ def test_batch_and_metropolis():
     dg = g.eval_shift_energy_batch(idx, disp)
     do = np.array([o.eval_shift_energy(i, *d) for i, d in zip(idx, disp)])
     assert np.abs(dg - do).max() <= ABS_DE
-    # sequential Metropolis: the oracle replays the same proposals
+    # sequential Metropolis: the oracle replays the same proposals; 300 moves
+    # run as two captured 128-move graphs plus 44 direct launches
+    m = 300
+    idx = rng.integers(0, 3000, m)
+    disp = rng.uniform(-0.5, 0.5, (m, 3))
     u = rng.uniform(0, 1, m)
     beta = 1.0
     dEg, accg = g.mc_run(idx, disp, u, beta)
