@@ -604,6 +604,18 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
     D.wprefix[l] = l <= maxref ? B.wprefix[l] : nullptr;
   }
   D.maxref = maxref;
+  D.level_start_d = d_level_start;
+  {
+    const void* ptrs[2 * MAX_LEVELS];
+    for (int l = 0; l < MAX_LEVELS; ++l) {
+      ptrs[l] = D.bm[l];
+      ptrs[MAX_LEVELS + l] = D.wprefix[l];
+    }
+    void** d_ptrs = static_cast<void**>(alloc(sizeof(ptrs)));
+    PDMK_CUDA(cudaMemcpyAsync(d_ptrs, ptrs, sizeof(ptrs), cudaMemcpyHostToDevice, st_));
+    D.bm_d = reinterpret_cast<const uint32_t* const*>(d_ptrs);
+    D.wprefix_d = reinterpret_cast<const int* const*>(d_ptrs + MAX_LEVELS);
+  }
   D.node_prefix = na.prefix;
   D.node_level = na.level;
   D.node_parent = na.parent;
@@ -820,6 +832,7 @@ void DmkTree::build_setup() {
   for (int l = 0; l < MAX_LEVELS + 2; ++l) D.dscale[l] = l >= 2 ? std::ldexp(1.0, -2 * (l - 2)) : 0.0;
   D.pw_lo = 2;
   D.pw_hi = D.max_depth - 2;  // may be < pw_lo: no difference levels
+  D.pw_base = D.level_start[D.pw_lo];
   // window_matrix (include/kernels.hpp:60-86)
   // The kernels depend on a mode only through m = ix^2 + iy^2 + iz^2 (in units
   // of dk), so psi_0 is evaluated once per distinct m.

@@ -247,7 +247,7 @@ __global__ void k_incoming(DevTree T, const int* __restrict__ boxes, int nboxes,
   const int X = compact3(p), Y = compact3(p >> 1), Z = compact3(p >> 2);
   const int n = T.n_diff, d = T.dd;
   const int k = tile * blockDim.x + threadIdx.x;
-  const int base = T.level_start[T.pw_lo];
+  const int base = T.pw_base;
   double e = 0;
   if (k < T.H) {
     const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
@@ -283,7 +283,7 @@ __global__ void k_tridot(DevTree T, const int* __restrict__ boxes, int nboxes, d
   const int tile = blockIdx.x / nboxes, b = blockIdx.x % nboxes;
   const int node = boxes[b];
   const int k = tile * blockDim.x + threadIdx.x;
-  const int base = T.level_start[T.pw_lo];
+  const int base = T.pw_base;
   double e = 0;
   if (k < T.H) {
     double2 o = T.out[size_t(node - base) * T.H + k];
@@ -314,7 +314,7 @@ __global__ void k_diff_finish(DevTree T, const int* __restrict__ boxes, int nbox
     int l = T.node_level[node];
     double t = 0;
     for (int tile = 0; tile < ktiles; ++tile) t += part[size_t(tile) * nboxes + b];
-    e += Cl[l] * T.dscale[l] * t - q2[b] * Sl[l];
+    e += Cl[l] * level_dscale(l) * t - q2[b] * Sl[l];
   }
   double s = block_sum(e, sm);
   if (threadIdx.x == 0) *out = s;
@@ -331,15 +331,6 @@ __global__ void k_window(DevTree T, double scale, double self, double* out) {
   if (threadIdx.x == 0) *out = s * scale - self;
 }
 
-// residual_kernel (include/kernels.hpp:50-58) with PolyFun::eval (include/pswf.hpp:70-78)
-__device__ inline double res_kernel(const DevTree& T, double r, double b) {
-  if (r == 0) return 0;
-  double xs = (r / b - 0.5) * 2.0;
-  if (fabs(xs) >= 1.0) return 0;
-  double v = 0;
-  for (int i = 0; i < T.n_poly; ++i) v = fma(v, xs, T.poly[i]);
-  return v / r;
-}
 
 __device__ inline int periodic_shift_d(double xi, double xj, double L, double bi, double bj) {
   if (xi < bi && xj > (L - bj)) return 1;
@@ -360,64 +351,88 @@ constexpr int RES_T = 128;
 constexpr int RES_CHUNK = 128;
 
 // leaf near field: 1/2 sum_{i in B} q_i sum_{j in N(B), j != i} q_j res(r_ij; bs_B)
+// (eval_energy_res, src/energy.cpp:82-173). The up to 35 source boxes (self,
+// colleagues, coarse-grain) are flattened into one index range: their
+// metadata is fetched in parallel, then sources are staged in chunks.
+template <int NP>
 __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __restrict__ leaves, double* part) {
   __shared__ double tx[RES_CHUNK], ty[RES_CHUNK], tz[RES_CHUNK], tq[RES_CHUNK];
   __shared__ double ux[RES_CHUNK], uy[RES_CHUNK], uz[RES_CHUNK], uq[RES_CHUNK];
+  __shared__ int uslot[RES_CHUNK];
+  __shared__ int m_beg[36], m_pre[37];
+  __shared__ double m_off[36][3];
   __shared__ double sm[32];
+  const ResidualPoly<NP> poly(T);
   const int node = leaves[blockIdx.x];
   const int l = T.node_level[node];
   const int cnt = T.leaf_count[node];
   double e = 0;
   if (l >= 2 && cnt > 0) {
-    const double b = T.boxsize[l];
-    double ci[3];
-    node_center(T, node, ci);
+    const double b = level_box(T, l);
     const int tb = T.node_begin[node];
+    if (threadIdx.x < 36) {
+      const int src = threadIdx.x;
+      int j = -1;
+      if (src == 0) j = node;
+      else if (src <= 27) j = (src - 1 == 13) ? -1 : T.col27[size_t(node) * 27 + (src - 1)];
+      else j = T.coarse8[size_t(node) * 8 + (src - 28)];
+      int beg = 0, n = 0;
+      double off[3] = {0, 0, 0};
+      if (j >= 0 && T.node_count[j] > 0) {
+        double ci[3], cj[3];
+        node_center(T, node, ci);
+        node_center(T, j, cj);
+        const double bj = level_box(T, T.node_level[j]);
+        for (int dd = 0; dd < 3; ++dd) off[dd] = -periodic_shift_d(ci[dd], cj[dd], T.L, b, bj) * T.L;
+        beg = T.node_begin[j];
+        n = (T.node_child0[j] < 0 ? beg + T.leaf_count[j] : T.node_end[j]) - beg;
+      }
+      m_beg[src] = beg;
+      m_pre[src] = n;
+      for (int dd = 0; dd < 3; ++dd) m_off[src][dd] = off[dd];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int s = 0;
+      for (int src = 0; src < 36; ++src) {
+        const int n = m_pre[src];
+        m_pre[src] = s;
+        s += n;
+      }
+      m_pre[36] = s;
+    }
+    __syncthreads();
+    const int total = m_pre[36];
     for (int t0 = 0; t0 < cnt; t0 += RES_CHUNK) {
       const int nt = min(RES_CHUNK, cnt - t0);
-      __syncthreads();
-      for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-        tx[t] = T.sx[tb + t0 + t];
-        ty[t] = T.sy[tb + t0 + t];
-        tz[t] = T.sz[tb + t0 + t];
-        tq[t] = T.sq[tb + t0 + t];
-      }
-      // sources: self, 26 colleagues, up to 8 coarse-grain neighbours
-      for (int src = 0; src < 35; ++src) {
-        int j;
-        if (src == 0) j = node;
-        else if (src <= 27) {
-          if (src - 1 == 13) continue;
-          j = T.col27[size_t(node) * 27 + (src - 1)];
-        } else {
-          j = T.coarse8[size_t(node) * 8 + (src - 28)];
+      for (int u0 = 0; u0 < total; u0 += RES_CHUNK) {
+        const int ns = min(RES_CHUNK, total - u0);
+        __syncthreads();
+        if (u0 == 0)
+          for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+            tx[t] = T.sx[tb + t0 + t];
+            ty[t] = T.sy[tb + t0 + t];
+            tz[t] = T.sz[tb + t0 + t];
+            tq[t] = T.sq[tb + t0 + t];
+          }
+        for (int t = threadIdx.x; t < ns; t += blockDim.x) {
+          const int ei = u0 + t;
+          int src = 0;
+          while (ei >= m_pre[src + 1]) ++src;
+          const int s = m_beg[src] + (ei - m_pre[src]);
+          ux[t] = T.sx[s] + m_off[src][0];
+          uy[t] = T.sy[s] + m_off[src][1];
+          uz[t] = T.sz[s] + m_off[src][2];
+          uq[t] = T.sq[s];
+          uslot[t] = src == 0 ? s : -1;
         }
-        if (j < 0 || T.node_count[j] == 0) continue;
-        double cj[3];
-        node_center(T, j, cj);
-        const double bj = T.boxsize[T.node_level[j]];
-        double off[3];
-        for (int dd = 0; dd < 3; ++dd) off[dd] = -periodic_shift_d(ci[dd], cj[dd], T.L, b, bj) * T.L;
-        const bool is_leaf = T.node_child0[j] < 0;
-        const int sb = T.node_begin[j];
-        const int se = is_leaf ? sb + T.leaf_count[j] : T.node_end[j];
-        for (int s0 = sb; s0 < se; s0 += RES_CHUNK) {
-          const int ns = min(RES_CHUNK, se - s0);
-          __syncthreads();
-          for (int t = threadIdx.x; t < ns; t += blockDim.x) {
-            ux[t] = T.sx[s0 + t] + off[0];
-            uy[t] = T.sy[s0 + t] + off[1];
-            uz[t] = T.sz[s0 + t] + off[2];
-            uq[t] = T.sq[s0 + t];
-          }
-          __syncthreads();
-          for (int pq = threadIdx.x; pq < nt * ns; pq += blockDim.x) {
-            int it = pq / ns, js = pq % ns;
-            if (src == 0 && s0 + js == tb + t0 + it) continue;
-            double dx = tx[it] - ux[js], dy = ty[it] - uy[js], dz = tz[it] - uz[js];
-            double r = sqrt(dx * dx + dy * dy + dz * dz);
-            if (r <= b) e += tq[it] * uq[js] * res_kernel(T, r, b);
-          }
+        __syncthreads();
+        for (int pq = threadIdx.x; pq < nt * ns; pq += blockDim.x) {
+          const int it = pq / ns, js = pq % ns;
+          if (uslot[js] == tb + t0 + it) continue;  // a particle with itself
+          const double dx = tx[it] - ux[js], dy = ty[it] - uy[js], dz = tz[it] - uz[js];
+          const double r = sqrt(dx * dx + dy * dy + dz * dz);
+          if (r <= b) e += tq[it] * uq[js] * poly(r, b);
         }
       }
     }
@@ -718,7 +733,9 @@ double DmkTree::eval_res_energy() {
   prepare_box_lists();
   DevTree& D = dev_;
   if (n_leaves_ > 0) {
-    k_residual<<<unsigned(n_leaves_), RES_T, 0, st_>>>(D, d_leaves_, D.partials);
+    auto kern = D.n_poly == 7 ? k_residual<7> : D.n_poly == 13 ? k_residual<13> : D.n_poly == 19 ? k_residual<19>
+                                                                                                 : k_residual<25>;
+    kern<<<unsigned(n_leaves_), RES_T, 0, st_>>>(D, d_leaves_, D.partials);
     PDMK_LAUNCH_CHECK();
     k_sum<<<1, 1024, 0, st_>>>(D.partials, n_leaves_, d_scalars_ + 2);
     PDMK_LAUNCH_CHECK();

@@ -32,8 +32,8 @@ constexpr int MAXLV = MAX_LEVELS;
 __device__ inline bool bm_get(const uint32_t* bm, uint64_t cell) { return (bm[cell >> 5] >> (cell & 31)) & 1u; }
 
 __device__ inline int bm_rank(const DevTree& T, int level, uint64_t cell) {
-  uint32_t w = T.bm[level][cell >> 5];
-  return T.wprefix[level][cell >> 5] + __popc(w & ((1u << (cell & 31)) - 1u));
+  uint32_t w = T.bm_d[level][cell >> 5];
+  return T.wprefix_d[level][cell >> 5] + __popc(w & ((1u << (cell & 31)) - 1u));
 }
 
 __device__ inline double center_of(double L, int l, int X) {
@@ -56,13 +56,6 @@ __device__ inline int periodic_shift_d(double xi, double xj, double L, double bi
   return 0;
 }
 
-__device__ inline double poly_res(const DevTree& T, double r, double b) {
-  double xs = (r / b - 0.5) * 2.0;
-  if (fabs(xs) >= 1.0) return 0;
-  double v = 0;
-  for (int i = 0; i < T.n_poly; ++i) v = fma(v, xs, T.poly[i]);
-  return v / r;
-}
 
 // Phase tables exp(-i m dk_l x) per axis for one point on its path. Layout:
 // root axes (3 x dw), then levels 2, 3, ... (3 x dd each). The accessors
@@ -135,7 +128,7 @@ __device__ void build_tables(const DevTree& T, const double* x, double q, const 
       int Xa = X[l][axis];
       int n = T.n_diff;
       int cnt = axis == 2 ? n + 1 : 2 * n + 1;
-      axis_table(x[axis] - center_of(T.L, l, Xa), T.delta_k[l], 1, Xa, n, cnt, axis == 2 ? q : 1.0,
+      axis_table(x[axis] - center_of(T.L, l, Xa), level_dk(T, l), 1, Xa, n, cnt, axis == 2 ? q : 1.0,
                  tb.lev[l][axis], part, NP);
     }
   }
@@ -187,11 +180,11 @@ __device__ void resolve(const DevTree& T, int i, const double* disp, Header& h) 
     int node = -1;
     if (l < T.max_depth) {
       const uint64_t cell = l == 0 ? 0 : key >> (3 * (KEY_BITS - l));
-      const bool exists = l <= 1 || bm_get(T.bm[l - 1], cell >> 3);
+      const bool exists = l <= 1 || bm_get(T.bm_d[l - 1], cell >> 3);
       if (exists) {
         node = l == 0 ? 0
-                      : (l == 1 ? 1 + int(cell) : T.level_start[l] + 8 * bm_rank(T, l - 1, cell >> 3) + int(cell & 7));
-        is_leaf = !(l <= T.maxref && bm_get(T.bm[l], cell));
+                      : (l == 1 ? 1 + int(cell) : T.level_start_d[l] + 8 * bm_rank(T, l - 1, cell >> 3) + int(cell & 7));
+        is_leaf = !(l <= T.maxref && bm_get(T.bm_d[l], cell));
       }
     }
     const unsigned leaves = (__ballot_sync(0xffffffffu, is_leaf) >> (16 * half)) & 0xffffu;
@@ -221,8 +214,10 @@ __device__ void resolve(const DevTree& T, int i, const double* disp, Header& h) 
 // q * sum_{j in N(leaf)} q_j res(|x - x_j|; bs_leaf), masked r^2 in (eps, b^2)
 // (eval_shift_energy_res_vec + direct_eval, src/energy_shift.cpp:233-302).
 // Source metadata is fetched in parallel, then all threads share the pairs.
-__device__ double residual_sum(const DevTree& T, int leaf, int l, const int* Xl, const double* x) {
-  const double b = T.boxsize[l];
+template <int NP>
+__device__ double residual_sum(const DevTree& T, const ResidualPoly<NP>& poly, int leaf, int l, const int* Xl,
+                               const double* x) {
+  const double b = level_box(T, l);
   const double b2 = b * b;
   const double eps = 2.220446049250313e-16;
   __shared__ int m_beg[36], m_cnt[36], m_pre[37], m_lvl[36];
@@ -244,7 +239,7 @@ __device__ double residual_sum(const DevTree& T, int leaf, int l, const int* Xl,
       beg = T.node_begin[j];
       const int end = ch < 0 ? beg + T.leaf_count[j] : T.node_end[j];
       cnt = end - beg;
-      const double bj = T.boxsize[lj];
+      const double bj = level_box(T, lj);
       const int Xj[3] = {int(compact3(pj)), int(compact3(pj >> 1)), int(compact3(pj >> 2))};
       for (int d = 0; d < 3; ++d)
         off[d] = -periodic_shift_d(center_of(T.L, l, Xl[d]), center_of(T.L, lj, Xj[d]), T.L, b, bj) * T.L;
@@ -274,7 +269,7 @@ __device__ double residual_sum(const DevTree& T, int leaf, int l, const int* Xl,
     const double dx = x[0] - (T.sx[s] + m_off[src][0]), dy = x[1] - (T.sy[s] + m_off[src][1]),
                  dz = x[2] - (T.sz[s] + m_off[src][2]);
     const double r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 > eps && r2 < b2) acc += T.sq[s] * poly_res(T, sqrt(r2), b);
+    if (r2 > eps && r2 < b2) acc += T.sq[s] * poly(sqrt(r2), b);
   }
   // arrivals parked in the overflow pool that belong to a source's subtree
   const int pn = *T.pool_n;
@@ -287,7 +282,7 @@ __device__ double residual_sum(const DevTree& T, int leaf, int l, const int* Xl,
     const double dx = x[0] - (T.px[p] + m_off[sj][0]), dy = x[1] - (T.py[p] + m_off[sj][1]),
                  dz = x[2] - (T.pz[p] + m_off[sj][2]);
     const double r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 > eps && r2 < b2) acc += T.pq[p] * poly_res(T, sqrt(r2), b);
+    if (r2 > eps && r2 < b2) acc += T.pq[p] * poly(sqrt(r2), b);
   }
   return acc;
 }
@@ -422,7 +417,7 @@ __device__ int build_receivers(const DevTree& T, const Header& h) {
   }
   __syncthreads();
   int pos = wsum[warp] + x - cnt;
-  const int base = T.level_start[T.pw_lo];
+  const int base = T.pw_base;
   for (int c = c0; c < min(c0 + per_thread, ncand); ++c) {
     if (!(ckey[c] >= 0 && (c < per || cmatch[c] < 0))) continue;
     const int r = c % per;
@@ -455,8 +450,7 @@ struct ShiftArgs {
   int mode;  // 0: evaluate only, 1: Metropolis
   double* dE_out;
   int* acc_out;
-  double c_window;            // dk_0^3 / (2 pi)^3
-  double c_level[MAXLV + 2];  // dk_l^3 / (2 pi)^3 * dscale_l
+  double c_window;  // dk_0^3 / (2 pi)^3
   double* partials;
   unsigned int* counter;
   Proposal* prop;
@@ -467,11 +461,19 @@ struct ShiftArgs {
 
 // Grid: blocks [0, G-2) do the plane-wave sums; block G-2 the target
 // residual, block G-1 the origin residual. The last block to finish reduces.
+template <int NP>
 __global__ void __launch_bounds__(SH_T) k_shift(DevTree T, ShiftArgs a) {
   extern __shared__ double2 sm2[];
   __shared__ Header h;
   __shared__ double red[4][32];
+  __shared__ double c_level[MAXLV + 2];  // dk_l^3 / (2 pi)^3 * dscale_l
   __shared__ bool is_last;
+  const ResidualPoly<NP> poly(T);
+  if (threadIdx.x >= 2 && threadIdx.x < MAXLV + 2) {
+    const double dk = level_dk(T, threadIdx.x);
+    c_level[threadIdx.x] = dk * dk * dk / (8.0 * 3.14159265358979323846 * 3.14159265358979323846 *
+                                           3.14159265358979323846) * level_dscale(threadIdx.x);
+  }
   if (a.cur) {
     const MoveCursor c = *a.cur;
     a.idx = c.idx;
@@ -524,7 +526,7 @@ __global__ void __launch_bounds__(SH_T) k_shift(DevTree T, ShiftArgs a) {
       acc[0] += (ar * br + ai * bi) * T.W[k];
     }
     // difference (src/energy_shift.cpp:92-140), all path levels per mode
-    const int base = T.level_start[T.pw_lo];
+    const int base = T.pw_base;
     const int d = T.dd;
     for (int k = t0; k < T.H; k += stride) {
       const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
@@ -532,21 +534,21 @@ __global__ void __launch_bounds__(SH_T) k_shift(DevTree T, ShiftArgs a) {
       for (int l = 2; l <= lo_max; ++l) {
         double2 o = cmul(oo.lev[l][2][iz], cmul(oo.lev[l][1][iy], oo.lev[l][0][ix]));
         double2 c = T.inc[size_t(h.path_o[l] - base) * T.H + k];
-        s -= (o.x * c.x - o.y * c.y - (o.x * o.x + o.y * o.y)) * a.c_level[l];
+        s -= (o.x * c.x - o.y * c.y - (o.x * o.x + o.y * o.y)) * c_level[l];
       }
       for (int l = 2; l <= lt_max; ++l) {
         double2 t = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
         double2 c = T.inc[size_t(h.path_t[l] - base) * T.H + k];
-        s += (t.x * c.x - t.y * c.y) * a.c_level[l];
+        s += (t.x * c.x - t.y * c.y) * c_level[l];
       }
       acc[1] += s * T.D2[k];
     }
   } else if (blockIdx.x == Gpw) {
     const int lt = h.depth_t - 1;
-    acc[2] = residual_sum(T, h.path_t[lt], lt, h.Xt[lt], h.xt) * h.q;
+    acc[2] = residual_sum(T, poly, h.path_t[lt], lt, h.Xt[lt], h.xt) * h.q;
   } else {
     const int lo = h.depth_o - 1;
-    acc[3] = residual_sum(T, h.path_o[lo], lo, h.Xo[lo], h.xo) * h.q;
+    acc[3] = residual_sum(T, poly, h.path_o[lo], lo, h.Xo[lo], h.xo) * h.q;
   }
   block_sum4(acc, red);
   if (threadIdx.x == 0) {
@@ -569,7 +571,7 @@ __global__ void __launch_bounds__(SH_T) k_shift(DevTree T, ShiftArgs a) {
     const double dEw = tot[0] * a.c_window;  // 2 * sum * dk0^3 / (2 (2 pi)^3)
     const double d = tot[1], rt = tot[2], ro = tot[3];
     double self = 0;
-    if (h.dr != 0) self = poly_res(T, h.dr, T.boxsize[2]) * h.q * h.q;
+    if (h.dr != 0) self = poly(h.dr, level_box(T, 2)) * h.q * h.q;
     const double dE = dEw + d + rt - ro - self;
     Proposal* P = a.prop;
     P->i_orig = h.i_orig;
@@ -695,7 +697,7 @@ __global__ void __launch_bounds__(UPD_T) k_update(DevTree T, const double2* __re
 
 // particle membership and position (exact on every level); one thread
 __device__ void commit_move(const DevTree& T) {
-  const Proposal P = *T.prop;
+  const Proposal& P = *T.prop;
   if (!P.accepted) return;
   const int leafA = P.path_o[P.depth_o - 1];
   const int leafB = P.path_t[P.depth_t - 1];
@@ -772,6 +774,18 @@ __device__ void commit_move(const DevTree& T) {
 }
 
 
+// the shift kernel for a residual polynomial of np coefficients (3, 6, 9, 12 digits)
+using ShiftKernel = void (*)(DevTree, ShiftArgs);
+ShiftKernel shift_kernel(int np) {
+  switch (np) {
+    case 7: return k_shift<7>;
+    case 13: return k_shift<13>;
+    case 19: return k_shift<19>;
+    case 25: return k_shift<25>;
+    default: throw std::invalid_argument("unsupported residual polynomial");
+  }
+}
+
 size_t tables_smem(const DevTree& T, int lmax, int copies) {
   size_t per = 3 * size_t(2 * T.n_window + 1) + size_t(std::max(lmax - 1, 0)) * 3 * (2 * T.n_diff + 1);
   return per * copies * sizeof(double2);
@@ -794,7 +808,6 @@ void DmkTree::launch_shift(const int* d_idx, const double* d_disp, const double*
   a.dE_out = d_dE;
   a.acc_out = d_acc;
   a.c_window = std::pow(D.delta_k[0], 3) / std::pow(2 * pi, 3);
-  for (int l = 0; l < MAX_LEVELS + 2; ++l) a.c_level[l] = std::pow(D.delta_k[l], 3) / std::pow(2 * pi, 3) * D.dscale[l];
   a.partials = D.partials;
   a.counter = D.counter;
   a.prop = D.prop;
@@ -804,7 +817,7 @@ void DmkTree::launch_shift(const int* d_idx, const double* d_disp, const double*
   a.ptab_per = ptab_per_;
   size_t smem = tables_smem(D, D.max_depth, 2);
   time_begin(0);
-  k_shift<<<unsigned(shift_grid_), SH_T, smem, st_>>>(D, a);
+  shift_kernel(D.n_poly)<<<unsigned(shift_grid_), SH_T, smem, st_>>>(D, a);
   PDMK_LAUNCH_CHECK();
   time_end(0);
 }
@@ -831,10 +844,11 @@ void DmkTree::ensure_move_resources() {
     PDMK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     shift_grid_ = 2 + sms;
     const size_t smem = tables_smem(D, D.max_depth, 2);
-    static size_t smem_set = 0;  // the attribute is per function, shared by all trees
-    if (smem > smem_set) {
-      PDMK_CUDA(cudaFuncSetAttribute(k_shift, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-      smem_set = smem;
+    static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
+    const int slot = (D.n_poly - 7) / 6;
+    if (smem > smem_set[slot]) {
+      PDMK_CUDA(cudaFuncSetAttribute(shift_kernel(D.n_poly), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      smem_set[slot] = smem;
     }
   }
 }

@@ -103,6 +103,12 @@ struct DevTree {
   const uint32_t* bm[MAX_LEVELS];
   const int* wprefix[MAX_LEVELS];
   int maxref;  // deepest level with a refined cell
+  // device copies of the per-level tables, for indexing by a run-time level
+  // (indexing the by-value kernel parameter would copy it to local memory)
+  const int* level_start_d;
+  const uint32_t* const* bm_d;
+  const int* const* wprefix_d;
+  int pw_base;  // level_start[pw_lo], the first node carrying expansions
   // expansions: root, then nodes of levels [pw_lo, pw_hi] (contiguous ids)
   double2* out_root;
   double2* out;  // [(node - level_start[pw_lo]) * H + k]
@@ -116,6 +122,34 @@ struct DevTree {
   Receiver* recv;  // [MAX_RECV]
   int* err;  // device error word (nonzero: pool overflow etc.)
   unsigned long long* work;  // [0] accepted moves, [1] update bytes (read + write)
+};
+
+// per-level geometry, computed rather than indexed: box side L 2^-l, the
+// difference-level mode spacing (2 pi / 3) / bs_l (form_wavenumbers,
+// src/tree.cpp:64-68) and the difference-kernel scale 4^-(l-2)
+__host__ __device__ inline double level_box(const DevTree& T, int l) { return ldexp(T.L, -l); }
+__host__ __device__ inline double level_dk(const DevTree& T, int l) {
+  return (2.0 * 3.14159265358979323846 / 3.0) / ldexp(T.L, -l);
+}
+__host__ __device__ inline double level_dscale(int l) { return ldexp(1.0, -2 * (l - 2)); }
+
+// The residual polynomial with its coefficients in registers (include/pswf.hpp:70-78
+// and include/kernels.hpp:50-58): res(r; b) = P(2 r / b - 1) / r, zero outside (0, b).
+template <int NP>
+struct ResidualPoly {
+  double c[NP];
+  __device__ explicit ResidualPoly(const DevTree& T) {
+#pragma unroll
+    for (int i = 0; i < NP; ++i) c[i] = T.poly[i];
+  }
+  __device__ double operator()(double r, double b) const {
+    const double xs = (r / b - 0.5) * 2.0;
+    if (fabs(xs) >= 1.0) return 0.0;
+    double v = 0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) v = fma(v, xs, c[i]);
+    return v / r;
+  }
 };
 
 struct EnergyParts {
