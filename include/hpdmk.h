@@ -131,6 +131,20 @@ int hpdmk_update_shift(hpdmk_tree tree, long i, double dx, double dy, double dz)
  * current state; no state change. Host arrays. */
 int hpdmk_eval_shift_energy_batch(hpdmk_tree tree, int m, const long *i, const double *d, double *dE);
 
+/* No reference counterpart. Same results as hpdmk_eval_shift_energy_batch, but
+ * the call allocates no device memory: its block partials, completion counter,
+ * proposal record, phase tables and staged inputs/outputs live in one fixed
+ * static device buffer (about 250 KB per device, found once per device). For
+ * callers that must not allocate once the tree exists.
+ * Limits: m <= HPDMK_STATIC_MAX_MOVES; larger m returns HPDMK_ERR_BAD_INPUT
+ * with a message and does no work. The buffer's completion counter must be
+ * zero at a launch: it is zero at load and every launch leaves it at zero.
+ * Calls that overlap in time on one device share the buffer and race: make
+ * them one after another. Make the first call on each device before any
+ * stream capture starts, since it looks up the buffer's address. */
+#define HPDMK_STATIC_MAX_MOVES 4096
+int hpdmk_eval_shift_energy_batch_static(hpdmk_tree tree, int m, const long *i, const double *d, double *dE);
+
 /* Batched extension: n sequential Metropolis moves at inverse temperature beta.
  * Move c proposes (i[c], d[3c..]) and is accepted when u[c] < exp(-beta dE);
  * accepted moves are committed before the next one. Outputs dE[c], accepted[c]

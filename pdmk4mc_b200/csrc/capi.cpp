@@ -256,6 +256,32 @@ int hpdmk_update_shift(hpdmk_tree t, long i, double dx, double dy, double dz) {
   });
 }
 
+int hpdmk_eval_shift_energy_batch_static(hpdmk_tree t, int m, const long* i, const double* d, double* dE) {
+  if (!t || m < 0 || (m > 0 && (!i || !d || !dE))) return fail(HPDMK_ERR_BAD_INPUT, "bad batch arguments");
+  if (m > HPDMK_STATIC_MAX_MOVES)
+    return fail(HPDMK_ERR_BAD_INPUT, "hpdmk_eval_shift_energy_batch_static: m = " + std::to_string(m) +
+                                         " exceeds the static buffer limit of " +
+                                         std::to_string(HPDMK_STATIC_MAX_MOVES) + " candidates per call");
+  Handle* h = H(t);
+  for (int c = 0; c < m; ++c)
+    if (check_move(h, i[c], d[3 * c], d[3 * c + 1], d[3 * c + 2]) != HPDMK_OK) return g_last_error;
+  if (m == 0) return ok();
+  return guarded([&]() {
+    // the scratch address is per device: make the tree's device current
+    int prev = 0;
+    PDMK_CUDA(cudaGetDevice(&prev));
+    if (prev != h->device) PDMK_CUDA(cudaSetDevice(h->device));
+    try {
+      h->tree->shift_batch_static(m, i, d, dE);
+    } catch (...) {
+      if (prev != h->device) cudaSetDevice(prev);
+      throw;
+    }
+    if (prev != h->device) PDMK_CUDA(cudaSetDevice(prev));
+    return ok();
+  });
+}
+
 int hpdmk_eval_shift_energy_batch(hpdmk_tree t, int m, const long* i, const double* d, double* dE) {
   if (!t || m < 0 || (m > 0 && (!i || !d || !dE))) return fail(HPDMK_ERR_BAD_INPUT, "bad batch arguments");
   Handle* h = H(t);

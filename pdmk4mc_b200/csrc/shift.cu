@@ -18,6 +18,8 @@
 // and the two paths are resolved by the lanes of one warp in parallel.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -838,6 +840,12 @@ void DmkTree::ensure_move_resources() {
     ptab_ = static_cast<double2*>(alloc(sizeof(double2) * 2 * size_t(ptab_per_)));
     d_cursor_ = static_cast<MoveCursor*>(alloc(sizeof(MoveCursor)));
   }
+  ensure_shift_config();
+}
+
+// Grid size and dynamic shared memory limit of the shift kernel (no allocation).
+void DmkTree::ensure_shift_config() {
+  DevTree& D = dev_;
   if (shift_grid_ == 0) {
     int dev = 0, sms = 148;
     PDMK_CUDA(cudaGetDevice(&dev));
@@ -1020,6 +1028,104 @@ void DmkTree::mc_run_device(int n_moves, const int* d_idx, const double* d_disp,
 
 void DmkTree::shift_batch_device(int m, const int* d_idx, const double* d_disp, double* d_dE) {
   for (int c = 0; c < m; ++c) launch_shift(d_idx, d_disp, nullptr, 0.0, c, 0, d_dE, nullptr);
+  last_valid_ = false;
+}
+
+
+// ---------------------------------------------------------------------------
+// Candidate batch through a fixed static device buffer. For callers that may
+// not allocate device memory once the tree exists (a pool-managed process, a
+// host thread that must not enter the allocator between steps): the block
+// partials, completion counter, proposal record, phase tables and the staged
+// inputs/outputs all live in g_static_scratch, whose address is looked up once
+// per device. The completion counter must be zero when a launch starts: the
+// buffer is zero at module load and every launch's last block sets it back.
+// Calls that overlap in time on one device (two host threads, two trees on
+// different streams) share the buffer and race; serialise them.
+namespace {
+constexpr int kStaticMaxMoves = 4096;   // candidates per call
+constexpr int kStaticMaxBlocks = 1024;  // shift grid (2 + SM count)
+constexpr long kStaticMaxTable = 2048;  // complex phase entries per path (digits <= 12 needs 2013)
+constexpr size_t kOffCounter = 0;
+constexpr size_t kOffPartials = 256;
+constexpr size_t kOffProp = kOffPartials + sizeof(double) * 4 * kStaticMaxBlocks;
+constexpr size_t kOffPtab = kOffProp + ((sizeof(Proposal) + 255) / 256) * 256;
+constexpr size_t kOffIdx = kOffPtab + sizeof(double2) * 2 * kStaticMaxTable;
+constexpr size_t kOffDisp = kOffIdx + sizeof(int) * kStaticMaxMoves;
+constexpr size_t kOffDE = kOffDisp + sizeof(double) * 3 * kStaticMaxMoves;
+constexpr size_t kStaticBytes = kOffDE + sizeof(double) * kStaticMaxMoves;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+unsigned char* static_scratch() {
+  static std::mutex mu;
+  static void* addr[64] = {};
+  int dev = 0;
+  PDMK_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw std::runtime_error("device ordinal out of range for the static scratch table");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || !p)
+      throw CudaError(std::string("cudaGetSymbolAddress(static shift scratch): ") + cudaGetErrorString(e));
+    addr[dev] = p;
+  }
+  return static_cast<unsigned char*>(addr[dev]);
+}
+}  // namespace
+
+void DmkTree::shift_batch_static(int m, const long* h_idx, const double* h_disp, double* h_dE) {
+  DevTree& D = dev_;
+  if (m < 0 || m > kStaticMaxMoves)
+    throw std::invalid_argument("static scratch holds at most " + std::to_string(kStaticMaxMoves) +
+                                " candidates per call, got " + std::to_string(m));
+  const long per = 3L * (2 * D.n_window + 1) + long(MAX_LEVELS + 1) * 3 * (2 * D.n_diff + 1);
+  if (per > kStaticMaxTable)
+    throw std::invalid_argument("phase tables of " + std::to_string(per) + " entries exceed the static scratch limit " +
+                                std::to_string(kStaticMaxTable));
+  if (m == 0) return;
+  ensure_shift_config();
+  if (shift_grid_ > kStaticMaxBlocks)
+    throw std::invalid_argument("shift grid of " + std::to_string(shift_grid_) +
+                                " blocks exceeds the static scratch limit " + std::to_string(kStaticMaxBlocks));
+  unsigned char* base = static_scratch();
+  int* s_idx = reinterpret_cast<int*>(base + kOffIdx);
+  double* s_disp = reinterpret_cast<double*>(base + kOffDisp);
+  double* s_dE = reinterpret_cast<double*>(base + kOffDE);
+  // indices narrowed through a stack buffer (pageable copies are staged
+  // before cudaMemcpyAsync returns, so the buffer may be reused at once)
+  int chunk[512];
+  for (int c0 = 0; c0 < m; c0 += 512) {
+    const int nc = std::min(512, m - c0);
+    for (int c = 0; c < nc; ++c) chunk[c] = int(h_idx[c0 + c]);
+    PDMK_CUDA(cudaMemcpyAsync(s_idx + c0, chunk, sizeof(int) * nc, cudaMemcpyHostToDevice, st_));
+  }
+  PDMK_CUDA(cudaMemcpyAsync(s_disp, h_disp, sizeof(double) * 3 * m, cudaMemcpyHostToDevice, st_));
+  const double pi = 3.14159265358979323846;
+  ShiftArgs a{};
+  a.idx = s_idx;
+  a.disp = s_disp;
+  a.u = nullptr;
+  a.beta = 0.0;
+  a.mode = 0;
+  a.dE_out = s_dE;
+  a.acc_out = nullptr;
+  a.c_window = std::pow(D.delta_k[0], 3) / std::pow(2 * pi, 3);
+  a.partials = reinterpret_cast<double*>(base + kOffPartials);
+  a.counter = reinterpret_cast<unsigned int*>(base + kOffCounter);
+  a.prop = reinterpret_cast<Proposal*>(base + kOffProp);
+  a.ptab = reinterpret_cast<double2*>(base + kOffPtab);
+  a.ptab_per = per;
+  a.cur = nullptr;
+  const size_t smem = tables_smem(D, D.max_depth, 2);
+  for (int c = 0; c < m; ++c) {
+    a.move = c;
+    shift_kernel(D.n_poly)<<<unsigned(shift_grid_), SH_T, smem, st_>>>(D, a);
+    PDMK_LAUNCH_CHECK();
+  }
+  PDMK_CUDA(cudaMemcpyAsync(h_dE, s_dE, sizeof(double) * m, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
   last_valid_ = false;
 }
 

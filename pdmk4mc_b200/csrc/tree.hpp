@@ -187,6 +187,9 @@ class DmkTree {
                      double* d_dE, int* d_acc);
   // batched energy shifts of many candidates against the current state
   void shift_batch_device(int m, const int* d_idx, const double* d_disp, double* d_dE);
+  // the same batch through one fixed static device buffer: no device
+  // allocation in the call (host arrays in and out, synchronous)
+  void shift_batch_static(int m, const long* h_idx, const double* h_disp, double* h_dE);
 
   // introspection (tests)
   int max_depth() const { return dev_.max_depth; }
@@ -279,6 +282,7 @@ class DmkTree {
   bool capturing_ = false;
   bool use_cursor_ = false;
   void ensure_move_resources();
+  void ensure_shift_config();
   void build_mc_graph(int timed);
   void launch_shift_cursor(int move);
   cudaStream_t aux_ = nullptr;  // second stream for the root plane-wave pass

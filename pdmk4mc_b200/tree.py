@@ -20,6 +20,7 @@ import numpy as np
 
 DIRECT = 1
 PROXY = 2
+STATIC_MAX_MOVES = 4096  # HPDMK_STATIC_MAX_MOVES in include/hpdmk.h
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -107,6 +108,8 @@ def load_library():
                                      ctypes.c_double]
     L.hpdmk_eval_shift_energy_batch.restype = ctypes.c_int
     L.hpdmk_eval_shift_energy_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp]
+    L.hpdmk_eval_shift_energy_batch_static.restype = ctypes.c_int
+    L.hpdmk_eval_shift_energy_batch_static.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp]
     L.hpdmk_mc_run.restype = ctypes.c_int
     L.hpdmk_mc_run.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp, ctypes.c_double, _dp, _ip]
     L.hpdmk_mc_run_device.restype = ctypes.c_int
@@ -242,6 +245,16 @@ class HPDMKPtTree:
         out = np.zeros(idx.size)
         _check(load_library().hpdmk_eval_shift_energy_batch(self._h, int(idx.size), _p(idx, _lp), _p(disp),
                                                             _p(out)))
+        return out
+
+    def eval_shift_energy_batch_static(self, idx, disp):
+        """eval_shift_energy_batch through the fixed static device buffer:
+        no device allocation in the call, at most STATIC_MAX_MOVES candidates."""
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        disp = np.ascontiguousarray(disp, dtype=np.float64).reshape(-1)
+        out = np.zeros(idx.size)
+        _check(load_library().hpdmk_eval_shift_energy_batch_static(self._h, int(idx.size), _p(idx, _lp), _p(disp),
+                                                                   _p(out)))
         return out
 
     def mc_run(self, idx, disp, u, beta):
