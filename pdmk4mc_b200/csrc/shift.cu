@@ -998,10 +998,12 @@ void DmkTree::update_shift(long i, double dx, double dy, double dz) {
 void DmkTree::mc_run_device(int n_moves, const int* d_idx, const double* d_disp, const double* d_u, double beta,
                             double* d_dE, int* d_acc) {
   ensure_move_resources();
-  const int timed = timing_ ? 1 : 0;
   int m = 0;
-  // whole batches run as one captured graph each
+  // whole batches run as one captured graph each; with timing on, one batch
+  // in kTimedEvery runs the graph variant whose updates are bracketed by
+  // event records (those records slow the graph, so only a sample carries them)
   while (n_moves - m >= kGraphMoves) {
+    const int timed = (timing_ && (timed_batches_++ % kTimedEvery) == 0) ? 1 : 0;
     if (!mc_graph_[timed]) build_mc_graph(timed);
     MoveCursor c{d_idx, d_disp, d_u, d_dE, d_acc, m, 1, beta};
     PDMK_CUDA(cudaMemcpyAsync(d_cursor_, &c, sizeof(c), cudaMemcpyHostToDevice, st_));

@@ -276,6 +276,8 @@ class DmkTree {
   int shift_grid_ = 0;
   // captured Metropolis batches (plain, and with per-update timing events)
   static constexpr int kGraphMoves = 128;
+  static constexpr int kTimedEvery = 8;
+  long timed_batches_ = 0;
   cudaGraphExec_t mc_graph_[2] = {nullptr, nullptr};
   std::vector<cudaEvent_t> graph_ev_;  // [2 * kGraphMoves] start/end of each update
   MoveCursor* d_cursor_ = nullptr;
