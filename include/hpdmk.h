@@ -181,6 +181,10 @@ int hpdmk_get_timing(hpdmk_tree tree, double *out, int reset);
  * expansion data read+written by their updates (algorithmic: 32 B per complex RMW). */
 int hpdmk_get_update_bytes(hpdmk_tree tree, double *out);
 
+/* Kernel launches this library has issued since it was loaded, kernels run
+ * inside its captured CUDA graphs included (no reference counterpart). */
+int hpdmk_get_launch_count(long long *out);
+
 /* Last status of the calling thread and its message. */
 int hpdmk_last_error(void);
 const char *hpdmk_last_error_message(void);

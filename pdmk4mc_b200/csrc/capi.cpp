@@ -380,6 +380,12 @@ int hpdmk_get_timing(hpdmk_tree t, double* out, int reset) {
   });
 }
 
+int hpdmk_get_launch_count(long long* out) {
+  if (!out) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  *out = pdmk::g_launch_count.load();
+  return ok();
+}
+
 int hpdmk_get_update_bytes(hpdmk_tree t, double* out) {
   if (!t || !out) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
   return guarded([&]() {

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -26,7 +27,14 @@ struct CudaError : std::runtime_error {
                               ":" + std::to_string(__LINE__));                                        \
   } while (0)
 
-#define PDMK_LAUNCH_CHECK() PDMK_CUDA(cudaGetLastError())
+// kernels this library has launched (graph-executed ones included)
+inline std::atomic<long long> g_launch_count{0};
+
+#define PDMK_LAUNCH_CHECK()                                  \
+  do {                                                       \
+    PDMK_CUDA(cudaGetLastError());                           \
+    ::pdmk::g_launch_count.fetch_add(1, std::memory_order_relaxed); \
+  } while (0)
 
 // ---------------------------------------------------------------------------
 // complex FP64 on double2

@@ -871,6 +871,7 @@ void DmkTree::build_mc_graph(int timed) {
     for (auto& e : graph_ev_) PDMK_CUDA(cudaEventCreate(&e));
   }
   cudaGraph_t g;
+  const long long launches0 = g_launch_count.load();  // captured launches do not run here
   capturing_ = true;
   PDMK_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   try {
@@ -887,6 +888,7 @@ void DmkTree::build_mc_graph(int timed) {
   }
   PDMK_CUDA(cudaStreamEndCapture(st_, &g));
   capturing_ = false;
+  g_launch_count.store(launches0);
   PDMK_CUDA(cudaGraphInstantiate(&mc_graph_[timed], g, 0));
   PDMK_CUDA(cudaGraphDestroy(g));
 }
@@ -1008,6 +1010,7 @@ void DmkTree::mc_run_device(int n_moves, const int* d_idx, const double* d_disp,
     MoveCursor c{d_idx, d_disp, d_u, d_dE, d_acc, m, 1, beta};
     PDMK_CUDA(cudaMemcpyAsync(d_cursor_, &c, sizeof(c), cudaMemcpyHostToDevice, st_));
     PDMK_CUDA(cudaGraphLaunch(mc_graph_[timed], st_));
+    g_launch_count.fetch_add(2 * kGraphMoves, std::memory_order_relaxed);  // shift + update per move
     if (timed) {
       // the events are reused by the next launch: read them now
       PDMK_CUDA(cudaStreamSynchronize(st_));

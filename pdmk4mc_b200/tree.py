@@ -62,6 +62,13 @@ def library_path() -> str:
     return os.environ.get("PDMK_B200_LIB", os.path.join(_HERE, "libhpdmk_b200.so"))
 
 
+def launch_count() -> int:
+    """Kernels this library has launched since it was loaded (graph-run ones included)."""
+    v = ctypes.c_longlong(0)
+    _check(load_library().hpdmk_get_launch_count(ctypes.byref(v)))
+    return int(v.value)
+
+
 def load_library():
     global _LIB
     if _LIB is not None:
@@ -86,6 +93,8 @@ def load_library():
     L.hpdmk_set_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.hpdmk_get_timing.restype = ctypes.c_int
     L.hpdmk_get_timing.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int]
+    L.hpdmk_get_launch_count.restype = ctypes.c_int
+    L.hpdmk_get_launch_count.argtypes = [ctypes.POINTER(ctypes.c_longlong)]
     L.hpdmk_get_update_bytes.restype = ctypes.c_int
     L.hpdmk_get_update_bytes.argtypes = [ctypes.c_void_p, _dp]
     L.hpdmk_tree_destroy.restype = None
