@@ -215,6 +215,7 @@ def run_b200(args, rank, ws):
     d_q = torch.tensor(q, dtype=torch.float64, device="cuda")
     # MC tree (slack for moves); its stream carries every kernel
     tree = P.HPDMKPtTree(params, r, q, leaf_slack=8)
+    tree.set_mc_mode(P.MC_GRAPH if args.mc_mode == "graph" else P.MC_PERSISTENT)
     stream = torch.cuda.ExternalStream(tree.stream_ptr())
     tree.form_outgoing_pw()
     tree.form_incoming_pw()
@@ -223,7 +224,7 @@ def run_b200(args, rank, ws):
 
     t_moves = []
     t_energy = []
-    work = np.zeros(2)
+    work = np.zeros(3)
     launches = 0
     l2_flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     clk_path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv") if os.path.isdir(
@@ -272,12 +273,20 @@ def run_b200(args, rank, ws):
     te = all_max(float(np.sum(t_energy)), ws)
     moves_per_s = ws * M * args.steps / tm
     energy_per_s = ws * args.steps / te
-    # roofline of the dominant MC kernel (the accept-and-update pair): HBM bound.
-    # Bytes per launch over every timed move; duration per launch from the
-    # event-bracketed sample of launches inside the timed region.
-    upd_ms, upd_n = timing["update"]
+    # roofline of the dominant MC kernel, HBM bound. Persistent mode: k_mc,
+    # one launch per step, bytes = dE reads + update read-modify-writes of all
+    # timed moves. Graph mode: k_update, bytes over every timed move, duration
+    # from the event-bracketed sample of launches inside the timed region.
     hbm, peak_kind = peaks()
-    bytes_per_launch = work[1] / (M * args.steps)
+    if args.mc_mode == "graph":
+        upd_ms, upd_n = timing["update"]
+        kernel = "k_update (accept-and-update; bytes averaged over all launches, rejected moves move none)"
+        bytes_per_launch = work[1] / (M * args.steps)
+    else:
+        upd_ms, upd_n = timing["mc"]
+        kernel = ("k_mc (persistent Metropolis: dE reads + accept-and-update read-modify-writes, "
+                  f"{M} moves per launch)")
+        bytes_per_launch = (work[1] + work[2]) / max(upd_n, 1)
     achieved = bytes_per_launch / (upd_ms / upd_n / 1e3) / 1e9 if upd_n else None
 
     # end to end through the C-ABI with host buffers (copies inside the timed region)
@@ -308,15 +317,14 @@ def run_b200(args, rank, ws):
             "metric": METRIC, "value": moves_per_s, "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * (tm + te) / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(W, parallelism="replicas" if ws > 1 else "single", l2="flushed before each step; "
-                           "the 1 GB expansion set exceeds L2"),
+            "config": dict(W, parallelism="replicas" if ws > 1 else "single", mc_mode=args.mc_mode,
+                           l2="256 MB written before each step; the 0.56 GB of expansions exceed the 126 MB L2"),
             "full_energy_evals_per_s": energy_per_s,
             "accept_rate": work[0] / (M * args.steps),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "traffic": None,
-                         "kernel": "k_update (accept-and-update; bytes averaged over all launches, "
-                                   "rejected moves move none)",
-                         "sampled_launches": int(upd_n),
+                         "kernel": kernel,
+                         "timed_launches": int(upd_n),
                          "peak_source": peak_kind},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "moves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -334,6 +342,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mc-mode", default="persistent", choices=["persistent", "graph"])
     ap.add_argument("--moves-per-step", type=int, default=WORKLOAD["moves_per_step"],
                     help="smaller values only for profiler runs; the reported workload uses the default")
     args = ap.parse_args()

@@ -67,7 +67,7 @@ typedef void *hpdmk_tree;
 #define HPDMK_ERR_BAD_INPUT 2      /* n < 1, null pointer, position outside [0,L), non-finite value, index out of range */
 #define HPDMK_ERR_CUDA 4           /* CUDA runtime failure (message via hpdmk_last_error_message) */
 #define HPDMK_ERR_OUT_OF_MEMORY 5  /* device allocation failed */
-#define HPDMK_ERR_DEVICE 6         /* device-side error word set (overflow pool exhausted) */
+#define HPDMK_ERR_DEVICE 6         /* device-side error word set (overflow pool exhausted, grid barrier wait gave up) */
 #define HPDMK_ERR_INTERNAL 7
 
 /* precision modes of hpdmk_tree_init_ext */
@@ -152,6 +152,15 @@ int hpdmk_eval_shift_energy_batch_static(hpdmk_tree tree, int m, const long *i, 
 int hpdmk_mc_run(hpdmk_tree tree, int n, const long *i, const double *d, const double *u, double beta, double *dE,
                  int *accepted);
 
+/* How hpdmk_mc_run / hpdmk_mc_run_device execute the sequence (no reference
+ * counterpart): HPDMK_MC_PERSISTENT (default) runs it as one cooperative
+ * launch on every SM with grid barriers between the phases of a move;
+ * HPDMK_MC_GRAPH runs CUDA graphs of 128 (shift, update) launch pairs.
+ * Both give the same results to rounding. */
+#define HPDMK_MC_PERSISTENT 0
+#define HPDMK_MC_GRAPH 1
+int hpdmk_set_mc_mode(hpdmk_tree tree, int mode);
+
 /* As hpdmk_mc_run with device-resident int32 indices and device outputs, enqueued on
  * the tree's stream without a host synchronisation (stream may be NULL for the default). */
 int hpdmk_mc_run_device(hpdmk_tree tree, int n, const int *d_i, const double *d_d, const double *d_u, double beta,
@@ -170,15 +179,18 @@ int hpdmk_synchronize(hpdmk_tree tree);
 /* The CUDA stream (cudaStream_t) all work of the tree is enqueued on. */
 int hpdmk_get_stream(hpdmk_tree tree, void **stream);
 
-/* Kernel timing: with enable != 0, CUDA events bracket every shift, update and
- * outgoing-expansion launch on the tree's stream. hpdmk_get_timing synchronises and
- * returns, per kernel class c (0 shift, 1 update pair, 2 commit, 3 outgoing NUDFT),
- * out[2c] = total milliseconds and out[2c+1] = number of launches since the last reset. */
+/* Kernel timing: with enable != 0, CUDA events bracket every shift, update,
+ * persistent Metropolis and outgoing-expansion launch on the tree's stream
+ * (graph-run updates: a 1-in-8 sample of the batches). hpdmk_get_timing
+ * synchronises and returns, per kernel class c (0 shift, 1 update, 2 persistent
+ * Metropolis launch, 3 outgoing NUDFT), out[2c] = total milliseconds and
+ * out[2c+1] = number of launches since the last reset. */
 int hpdmk_set_timing(hpdmk_tree tree, int enable);
 int hpdmk_get_timing(hpdmk_tree tree, double *out, int reset);
 
 /* Work counters of the last MC batch: out[0] accepted moves, out[1] bytes of
- * expansion data read+written by their updates (algorithmic: 32 B per complex RMW). */
+ * expansion data read+written by their updates (algorithmic: 32 B per complex RMW),
+ * out[2] algorithmic bytes read by the dE evaluations of the persistent kernel. */
 int hpdmk_get_update_bytes(hpdmk_tree tree, double *out);
 
 /* Kernel launches this library has issued since it was loaded, kernels run

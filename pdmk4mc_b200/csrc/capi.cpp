@@ -94,6 +94,12 @@ int guarded(F&& f) {
 
 Handle* H(hpdmk_tree t) { return static_cast<Handle*>(t); }
 
+// device error word: bit 0 overflow pool exhausted, bit 1 grid barrier wait gave up
+int device_fail(int e) {
+  if (e & 2) return fail(HPDMK_ERR_DEVICE, "persistent Metropolis kernel: a grid barrier wait gave up");
+  return fail(HPDMK_ERR_DEVICE, "overflow pool exhausted");
+}
+
 int check_params(const HPDMKParams& p) {
   if (!(p.L > 0) || !std::isfinite(p.L)) return fail(HPDMK_ERR_BAD_PARAMS, "L must be positive and finite");
   if (p.n_per_leaf < 1) return fail(HPDMK_ERR_BAD_PARAMS, "n_per_leaf must be >= 1");
@@ -251,7 +257,7 @@ int hpdmk_update_shift(hpdmk_tree t, long i, double dx, double dy, double dz) {
   if (check_move(H(t), i, dx, dy, dz) != HPDMK_OK) return g_last_error;
   return guarded([&]() {
     H(t)->tree->update_shift(i, dx, dy, dz);
-    if (H(t)->tree->check_device_error()) return fail(HPDMK_ERR_DEVICE, "overflow pool exhausted");
+    if (int e = H(t)->tree->check_device_error()) return device_fail(e);
     return ok();
   });
 }
@@ -318,7 +324,7 @@ int hpdmk_mc_run(hpdmk_tree t, int n, const long* i, const double* d, const doub
     if (dE) PDMK_CUDA(cudaMemcpyAsync(dE, h->d_dE, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
     if (accepted) PDMK_CUDA(cudaMemcpyAsync(accepted, h->d_acc, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
     PDMK_CUDA(cudaStreamSynchronize(h->stream));
-    if (h->tree->check_device_error()) return fail(HPDMK_ERR_DEVICE, "overflow pool exhausted");
+    if (int e = h->tree->check_device_error()) return device_fail(e);
     return ok();
   });
 }
@@ -363,6 +369,13 @@ int hpdmk_synchronize(hpdmk_tree t) {
 int hpdmk_get_stream(hpdmk_tree t, void** stream) {
   if (!t || !stream) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
   *stream = static_cast<void*>(H(t)->stream);
+  return ok();
+}
+
+int hpdmk_set_mc_mode(hpdmk_tree t, int mode) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  if (mode != HPDMK_MC_PERSISTENT && mode != HPDMK_MC_GRAPH) return fail(HPDMK_ERR_BAD_PARAMS, "unknown mc mode");
+  H(t)->tree->set_mc_mode(mode);
   return ok();
 }
 

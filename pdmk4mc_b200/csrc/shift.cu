@@ -147,22 +147,31 @@ __device__ inline double2 phase_at(const A& ax, int k, int d) {
 // (one image per lane, src/energy_shift.cpp:30-41) and both leaf paths
 // (lanes 0-15 the target, 16-31 the origin, one level per lane, from the
 // refinement bitmaps: the reference's locate_particle, src/tree.cpp:204-236).
+// Loads of data that other blocks of a persistent kernel write (CG = true)
+// bypass L1, which is not coherent across SMs.
+template <bool CG, class V>
+__device__ inline V ldm(const V* p) {
+  if constexpr (CG) return __ldcg(p);
+  else return *p;
+}
+
+template <bool CG = false>
 __device__ void resolve(const DevTree& T, int i, const double* disp, Header& h) {
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
-    const int s = T.orig_slot[i];
+    const int s = ldm<CG>(T.orig_slot + i);
     double xo[3], q;
     if (s < T.n_slots) {
-      xo[0] = T.sx[s];
-      xo[1] = T.sy[s];
-      xo[2] = T.sz[s];
-      q = T.sq[s];
+      xo[0] = ldm<CG>(T.sx + s);
+      xo[1] = ldm<CG>(T.sy + s);
+      xo[2] = ldm<CG>(T.sz + s);
+      q = ldm<CG>(T.sq + s);
     } else {
       const int p = s - T.n_slots;
-      xo[0] = T.px[p];
-      xo[1] = T.py[p];
-      xo[2] = T.pz[p];
-      q = T.pq[p];
+      xo[0] = ldm<CG>(T.px + p);
+      xo[1] = ldm<CG>(T.py + p);
+      xo[2] = ldm<CG>(T.pz + p);
+      q = ldm<CG>(T.pq + p);
     }
     const double L = T.L;
     const double d0 = disp[0], d1 = disp[1], d2 = disp[2];
@@ -319,7 +328,7 @@ __device__ inline int dir_of_slot(int s) { return (s - 2) + ((s - 2) >= 13 ? 1 :
 // update needs a single launch without write races. Receivers are matched by
 // box coordinates (known from the header), the records go to T.recv and the
 // count is returned to every thread. Block-cooperative.
-__device__ int build_receivers(const DevTree& T, const Header& h) {
+__device__ int build_receivers(const DevTree& T, const Header& h, Receiver* out) {
   constexpr int PER = 28 * MAXLV;
   __shared__ int ckey[2 * PER];  // receiving node (-1 none)
   __shared__ signed char cfl[2 * PER][3];
@@ -436,7 +445,7 @@ __device__ int build_receivers(const DevTree& T, const Header& h) {
       R.fo[q] = is_t ? (m >= 0 ? cfl[m][q] : 0) : cfl[c][q];
     }
     R.pad[0] = R.pad[1] = 0;
-    T.recv[pos++] = R;
+    out[pos++] = R;
   }
   const int total = wsum[31];
   __syncthreads();
@@ -568,7 +577,7 @@ __global__ void __launch_bounds__(SH_T) k_shift(DevTree T, ShiftArgs a) {
   for (int b = threadIdx.x; b < G; b += blockDim.x)
     for (int c = 0; c < 4; ++c) tot[c] += __ldcg(a.partials + 4 * size_t(b) + c);
   block_sum4(tot, red);
-  const int nrecv = build_receivers(T, h);
+  const int nrecv = build_receivers(T, h, T.recv);
   if (threadIdx.x == 0) {
     const double dEw = tot[0] * a.c_window;  // 2 * sum * dk0^3 / (2 (2 pi)^3)
     const double d = tot[1], rt = tot[2], ro = tot[3];
@@ -618,7 +627,7 @@ __global__ void __launch_bounds__(SH_T) k_shift(DevTree T, ShiftArgs a) {
 constexpr int UPD_T = 128;
 constexpr int UPD_UNROLL = 8;
 
-__device__ void commit_move(const DevTree& T);
+__device__ void commit_move(const DevTree& T, const Proposal& P);
 
 __device__ inline double2 image_phase(double2 p, const signed char* f, int ix, int iy, int iz, int n, int two_l) {
   if (f[0] | f[1] | f[2]) {
@@ -643,7 +652,7 @@ __global__ void __launch_bounds__(UPD_T) k_update(DevTree T, const double2* __re
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
     atomicAdd(&T.work[0], 1ull);
     atomicAdd(&T.work[1], 32ull * ((unsigned long long)T.Hw + (unsigned long long)nr * T.H));
-    commit_move(T);
+    commit_move(T, *T.prop);
   }
   __syncthreads();
   Tables tt, to;
@@ -698,8 +707,7 @@ __global__ void __launch_bounds__(UPD_T) k_update(DevTree T, const double2* __re
 }
 
 // particle membership and position (exact on every level); one thread
-__device__ void commit_move(const DevTree& T) {
-  const Proposal& P = *T.prop;
+__device__ void commit_move(const DevTree& T, const Proposal& P) {
   if (!P.accepted) return;
   const int leafA = P.path_o[P.depth_o - 1];
   const int leafB = P.path_t[P.depth_t - 1];
@@ -775,6 +783,359 @@ __device__ void commit_move(const DevTree& T) {
   for (int l = 0; l < P.depth_t; ++l) T.node_count[P.path_t[l]] += 1;
 }
 
+
+// ---------------------------------------------------------------------------
+// Persistent Metropolis kernel: one cooperative launch runs a whole sequence
+// of trial moves on every SM. Per move, every block resolves the proposal and
+// builds both paths' phase tables itself (no broadcast needed), adds its share
+// of the window, difference and near-field sums, and publishes 4 partials;
+// after a grid barrier every block reduces all partials in the same fixed
+// order, so all blocks reach the same dE and the same Metropolis decision. An
+// accepted move is then applied by all blocks (receivers listed per block,
+// one read-modify-write per mode and vector), block 0 commits the particle,
+// and a second barrier orders the update before the next move. Barrier waits
+// are bounded; a wait that gives up sets an error bit and every block returns.
+constexpr int MC_T = 512;
+
+struct McArgs {
+  const int* idx;
+  const double* disp;
+  const double* u;
+  double beta;
+  int n_moves;
+  double* dE_out;
+  int* acc_out;
+  double c_window;          // dk_0^3 / (2 pi)^3
+  double* partials;         // [2][G][4], double-buffered by move parity
+  unsigned int* arrivals;   // barrier arrivals, zero at launch
+  long long spin_limit;     // polls before a barrier wait gives up
+};
+
+__device__ inline unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid barrier over a monotonically increasing arrival counter; nbar counts
+// the barriers this block has passed (kept by thread 0). False when the wait
+// gave up or another block reported a failure.
+__device__ bool mc_barrier(const DevTree& T, const McArgs& a, unsigned& nbar) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ++nbar;
+    const unsigned target = nbar * gridDim.x;
+    __threadfence();
+    atomicAdd(a.arrivals, 1u);
+    int ok = 1;
+    for (long long it = 0;; ++it) {
+      if (ld_acquire(a.arrivals) >= target) break;
+      if (ldm<true>(T.err) & 2) {
+        ok = 0;
+        break;
+      }
+      if (it >= a.spin_limit) {
+        atomicOr(T.err, 2);
+        ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Source lists of one path's leaf for the near field: the leaf, its 26
+// colleagues and 8 coarse neighbours, with their periodic offsets.
+struct ResMeta {
+  int beg[36], cnt[36], pre[37], lvl[36];
+  unsigned long long pfx[36];
+  double off[36][3];
+};
+
+__device__ void res_meta(const DevTree& T, int leaf, int l, const int* Xl, int src, ResMeta& M) {
+  const double b = level_box(T, l);
+  int j = -1;
+  if (src == 0) j = leaf;
+  else if (src <= 27) j = (src - 1 == 13) ? -1 : T.col27[size_t(leaf) * 27 + (src - 1)];
+  else j = T.coarse8[size_t(leaf) * 8 + (src - 28)];
+  int beg = 0, cnt = 0, lj = 0;
+  unsigned long long pj = 0;
+  double off[3] = {0, 0, 0};
+  if (j >= 0) {
+    lj = T.node_level[j];
+    pj = T.node_prefix[j];
+    const int ch = T.node_child0[j];
+    beg = T.node_begin[j];
+    const int end = ch < 0 ? beg + ldm<true>(T.leaf_count + j) : T.node_end[j];
+    cnt = end - beg;
+    const double bj = level_box(T, lj);
+    const int Xj[3] = {int(compact3(pj)), int(compact3(pj >> 1)), int(compact3(pj >> 2))};
+    for (int d = 0; d < 3; ++d)
+      off[d] = -periodic_shift_d(center_of(T.L, l, Xl[d]), center_of(T.L, lj, Xj[d]), T.L, b, bj) * T.L;
+  }
+  M.beg[src] = beg;
+  M.cnt[src] = j >= 0 ? cnt : -1;
+  M.lvl[src] = lj;
+  M.pfx[src] = pj;
+  for (int d = 0; d < 3; ++d) M.off[src][d] = off[d];
+}
+
+template <int NP>
+__global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
+  extern __shared__ double2 sm2[];
+  __shared__ Header h;
+  __shared__ double red[4][32];
+  __shared__ double c_level[MAXLV + 2];
+  __shared__ ResMeta meta[2];
+  __shared__ Receiver rs[MAX_RECV];
+  __shared__ Proposal P;
+  __shared__ int s_acc;
+  const ResidualPoly<NP> poly(T);
+  if (threadIdx.x >= 2 && threadIdx.x < MAXLV + 2) {
+    const double dk = level_dk(T, threadIdx.x);
+    c_level[threadIdx.x] = dk * dk * dk / (8.0 * 3.14159265358979323846 * 3.14159265358979323846 *
+                                           3.14159265358979323846) * level_dscale(threadIdx.x);
+  }
+  const int G = gridDim.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gstride = G * blockDim.x;
+  unsigned nbar = 0;
+  for (int m = 0; m < a.n_moves; ++m) {
+    resolve<true>(T, a.idx[m], a.disp + 3 * m, h);
+    const int lo_max = h.depth_o - 2, lt_max = h.depth_t - 2;
+    const int uo = min(h.depth_o - 1, T.pw_hi), ut = min(h.depth_t - 1, T.pw_hi);
+    const int per = 3 * (2 * T.n_window + 1) + max(max(uo, ut) - 1, 0) * 3 * (2 * T.n_diff + 1);
+    Tables to, oo;
+    alloc_tables(sm2, T, oo);
+    alloc_tables(sm2 + per, T, to);
+    // near-field source lists on threads 0..71, phase tables on the rest
+    if (threadIdx.x < 72) {
+      const int p = threadIdx.x / 36, src = threadIdx.x % 36;
+      const int lv = (p == 0 ? h.depth_t : h.depth_o) - 1;
+      res_meta(T, p == 0 ? h.path_t[lv] : h.path_o[lv], lv, p == 0 ? h.Xt[lv] : h.Xo[lv], src, meta[p]);
+    } else {
+      const int NPT = 4, nthr = blockDim.x - 72, t = threadIdx.x - 72;
+      for (int path = 0; path < 2; ++path) {
+        const int lmax = path == 0 ? uo : ut;
+        const int nlev = lmax >= 2 ? lmax - 1 : 0;
+        const int ntask = (1 + nlev) * 3 * NPT;
+        const double* x = path == 0 ? h.xo : h.xt;
+        const int(*X)[3] = path == 0 ? h.Xo : h.Xt;
+        const Tables& tb = path == 0 ? oo : to;
+        for (int k = t; k < ntask; k += nthr) {
+          const int part = k % NPT, axis = (k / NPT) % 3, slot = k / (3 * NPT);
+          if (slot == 0) {
+            const int n = T.n_window, cnt = axis == 2 ? n + 1 : 2 * n + 1;
+            axis_table(x[axis] - 0.5 * T.L, T.delta_k[0], 3, 0, n, cnt, axis == 2 ? h.q : 1.0, tb.root[axis], part,
+                       NPT);
+          } else {
+            const int l = slot + 1, Xa = X[l][axis], n = T.n_diff, cnt = axis == 2 ? n + 1 : 2 * n + 1;
+            axis_table(x[axis] - center_of(T.L, l, Xa), level_dk(T, l), 1, Xa, n, cnt, axis == 2 ? h.q : 1.0,
+                       tb.lev[l][axis], part, NPT);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      ResMeta& M = meta[threadIdx.x];
+      int s = 0;
+      for (int src = 0; src < 36; ++src) {
+        M.pre[src] = s;
+        s += max(M.cnt[src], 0);
+      }
+      M.pre[36] = s;
+    }
+    __syncthreads();
+    double acc[4] = {0, 0, 0, 0};
+    // window (src/energy_shift.cpp:72-90)
+    for (int k = gt; k < T.Hw; k += gstride) {
+      const double2 t = phase_at(to.root, k, T.dw), o = phase_at(oo.root, k, T.dw);
+      const double2 g = __ldcg(T.out_root + k);
+      const double ar = t.x - o.x, ai = t.y - o.y, br = g.x - o.x, bi = g.y - o.y;
+      acc[0] += (ar * br + ai * bi) * T.W[k];
+    }
+    // difference (src/energy_shift.cpp:92-140)
+    {
+      const int base = T.pw_base, d = T.dd;
+      for (int k = gt; k < T.H; k += gstride) {
+        const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
+        double s = 0;
+        for (int l = 2; l <= lo_max; ++l) {
+          const double2 o = cmul(oo.lev[l][2][iz], cmul(oo.lev[l][1][iy], oo.lev[l][0][ix]));
+          const double2 c = __ldcg(T.inc + size_t(h.path_o[l] - base) * T.H + k);
+          s -= (o.x * c.x - o.y * c.y - (o.x * o.x + o.y * o.y)) * c_level[l];
+        }
+        for (int l = 2; l <= lt_max; ++l) {
+          const double2 t = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
+          const double2 c = __ldcg(T.inc + size_t(h.path_t[l] - base) * T.H + k);
+          s += (t.x * c.x - t.y * c.y) * c_level[l];
+        }
+        acc[1] += s * T.D2[k];
+      }
+    }
+    // near field of the target and the origin (src/energy_shift.cpp:233-302):
+    // the pairs of both paths split evenly over the blocks
+    {
+      const int nt = meta[0].pre[36], no = meta[1].pre[36], np = nt + no;
+      const int e0 = int((long(blockIdx.x) * np) / G), e1 = int((long(blockIdx.x + 1) * np) / G);
+      const double eps = 2.220446049250313e-16;
+      for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const int p = e < nt ? 0 : 1;
+        const ResMeta& M = meta[p];
+        const int ee = p == 0 ? e : e - nt;
+        int src = 0;
+        while (ee >= M.pre[src + 1]) ++src;
+        const int lv = (p == 0 ? h.depth_t : h.depth_o) - 1;
+        const double b = level_box(T, lv);
+        const double* x = p == 0 ? h.xt : h.xo;
+        const int s = M.beg[src] + (ee - M.pre[src]);
+        const double dx = x[0] - (__ldcg(T.sx + s) + M.off[src][0]), dy = x[1] - (__ldcg(T.sy + s) + M.off[src][1]),
+                     dz = x[2] - (__ldcg(T.sz + s) + M.off[src][2]);
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 > eps && r2 < b * b) acc[2 + p] += __ldcg(T.sq + s) * poly(sqrt(r2), b);
+      }
+      // arrivals parked in the overflow pool that belong to a source's subtree
+      const int pn = __ldcg(T.pool_n);
+      for (int e = gt; e < 2 * 36 * pn; e += gstride) {
+        const int p = e / (36 * pn), sj = (e / pn) % 36, q = e % pn;
+        const ResMeta& M = meta[p];
+        if (M.cnt[sj] < 0 || __ldcg(T.p_orig + q) < 0) continue;
+        const int pl = __ldcg(T.p_leaf + q);
+        const int ll = T.node_level[pl], lj = M.lvl[sj];
+        if (ll < lj || (T.node_prefix[pl] >> (3 * (ll - lj))) != M.pfx[sj]) continue;
+        const int lv = (p == 0 ? h.depth_t : h.depth_o) - 1;
+        const double b = level_box(T, lv);
+        const double* x = p == 0 ? h.xt : h.xo;
+        const double dx = x[0] - (__ldcg(T.px + q) + M.off[sj][0]), dy = x[1] - (__ldcg(T.py + q) + M.off[sj][1]),
+                     dz = x[2] - (__ldcg(T.pz + q) + M.off[sj][2]);
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 > eps && r2 < b * b) acc[2 + p] += __ldcg(T.pq + q) * poly(sqrt(r2), b);
+      }
+      acc[2] *= h.q;
+      acc[3] *= h.q;
+    }
+    block_sum4(acc, red);
+    double* part = a.partials + size_t(m & 1) * 4 * G;
+    if (threadIdx.x == 0)
+      for (int c = 0; c < 4; ++c) part[4 * blockIdx.x + c] = acc[c];
+    if (!mc_barrier(T, a, nbar)) return;
+    // every block reduces the same partials in the same order
+    double tot[4] = {0, 0, 0, 0};
+    for (int b = threadIdx.x; b < G; b += blockDim.x)
+      for (int c = 0; c < 4; ++c) tot[c] += __ldcg(part + 4 * b + c);
+    block_sum4(tot, red);
+    if (threadIdx.x == 0) {
+      const double dEw = tot[0] * a.c_window;
+      double self = 0;
+      if (h.dr != 0) self = poly(h.dr, level_box(T, 2)) * h.q * h.q;
+      const double dE = dEw + tot[1] + tot[2] - tot[3] - self;
+      const int accd = a.u[m] < exp(-a.beta * dE) ? 1 : 0;
+      s_acc = accd;
+      if (blockIdx.x == 0) {
+        if (a.dE_out) a.dE_out[m] = dE;
+        if (a.acc_out) a.acc_out[m] = accd;
+        // algorithmic bytes of the dE evaluation: root and incoming rows, W and
+        // D, 32 B per near-field source particle
+        const int nlev = max(lo_max - 1, 0) + max(lt_max - 1, 0);
+        atomicAdd(&T.work[2], 24ull * T.Hw + 16ull * nlev * T.H + 8ull * T.H +
+                                  32ull * (unsigned long long)(meta[0].pre[36] + meta[1].pre[36]));
+      }
+    }
+    __syncthreads();
+    if (!s_acc) continue;
+    // accept-and-update (src/tree.cpp:447-597)
+    const int nr = build_receivers(T, h, rs);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      P.i_orig = h.i_orig;
+      P.slot = h.slot;
+      P.q = h.q;
+      for (int c = 0; c < 3; ++c) {
+        P.xo[c] = h.xo[c];
+        P.xt[c] = h.xt[c];
+      }
+      P.depth_o = h.depth_o;
+      P.depth_t = h.depth_t;
+      for (int l = 0; l < MAXLV; ++l) {
+        P.path_o[l] = l < h.depth_o ? h.path_o[l] : -1;
+        P.path_t[l] = l < h.depth_t ? h.path_t[l] : -1;
+      }
+      P.accepted = 1;
+      P.valid = 1;
+      P.n_recv = nr;
+      atomicAdd(&T.work[0], 1ull);
+      atomicAdd(&T.work[1], 32ull * ((unsigned long long)T.Hw + (unsigned long long)nr * T.H));
+      commit_move(T, P);
+    }
+    {
+      const int Hk = ((max(T.H, T.Hw) + 31) / 32) * 32;
+      const int ng = max(1, min(8, gstride / Hk));
+      const int n = T.n_diff, d = T.dd;
+      for (int item = gt; item < Hk * ng; item += gstride) {
+        const int k = item % Hk, rg = item / Hk;
+        if (rg == 0 && k < T.Hw) {
+          const double2 t = phase_at(to.root, k, T.dw), o = phase_at(oo.root, k, T.dw);
+          double2 g = __ldcg(T.out_root + k);
+          g = cadd(g, t);
+          g = csub(g, o);
+          T.out_root[k] = g;
+        }
+        if (k >= T.H) continue;
+        const int r0 = (rg * nr) / ng, r1 = ((rg + 1) * nr) / ng;
+        const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
+        int r = r0;
+        while (r < r1) {
+          const int l = rs[r].level;
+          int re = r + 1;
+          while (re < r1 && rs[re].level == l) ++re;
+          const double2 pt = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
+          const double2 po = cmul(oo.lev[l][2][iz], cmul(oo.lev[l][1][iy], oo.lev[l][0][ix]));
+          const int two_l = (l & 1) ? 2 : 1;
+          for (; r < re; r += UPD_UNROLL) {
+            double2 v[UPD_UNROLL];
+            size_t off[UPD_UNROLL];
+#pragma unroll
+            for (int q = 0; q < UPD_UNROLL; ++q) {
+              if (r + q < re) {
+                const Receiver& R = rs[r + q];
+                off[q] = size_t(R.off) * T.H + k;
+                v[q] = R.is_out ? __ldcg(T.out + off[q]) : __ldcg(T.inc + off[q]);
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < UPD_UNROLL; ++q) {
+              if (r + q < re) {
+                const Receiver& R = rs[r + q];
+                double2 del = make_double2(0.0, 0.0);
+                if (R.has_t) del = image_phase(pt, R.ft, ix, iy, iz, n, two_l);
+                if (R.has_o) del = csub(del, image_phase(po, R.fo, ix, iy, iz, n, two_l));
+                if (R.is_out) T.out[off[q]] = cadd(v[q], del);
+                else T.inc[off[q]] = make_double2(v[q].x + del.x, v[q].y - del.y);
+              }
+            }
+          }
+          r = re;
+        }
+      }
+    }
+    if (!mc_barrier(T, a, nbar)) return;
+  }
+}
+
+using McKernel = void (*)(DevTree, McArgs);
+McKernel mc_kernel(int np) {
+  switch (np) {
+    case 7: return k_mc<7>;
+    case 13: return k_mc<13>;
+    case 19: return k_mc<19>;
+    case 25: return k_mc<25>;
+    default: throw std::invalid_argument("unsupported residual polynomial");
+  }
+}
 
 // the shift kernel for a residual polynomial of np coefficients (3, 6, 9, 12 digits)
 using ShiftKernel = void (*)(DevTree, ShiftArgs);
@@ -956,14 +1317,13 @@ void DmkTree::get_timing(double* out, bool reset) {
 }
 
 void DmkTree::get_work(double* out) {
-  unsigned long long w[2];
+  unsigned long long w[3];
   PDMK_CUDA(cudaMemcpyAsync(w, dev_.work, sizeof(w), cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaStreamSynchronize(st_));
-  out[0] = double(w[0]);
-  out[1] = double(w[1]);
+  for (int c = 0; c < 3; ++c) out[c] = double(w[c]);
 }
 
-void DmkTree::reset_work() { PDMK_CUDA(cudaMemsetAsync(dev_.work, 0, 2 * sizeof(unsigned long long), st_)); }
+void DmkTree::reset_work() { PDMK_CUDA(cudaMemsetAsync(dev_.work, 0, 3 * sizeof(unsigned long long), st_)); }
 
 double DmkTree::eval_shift_energy(long i, double dx, double dy, double dz, double* parts) {
   double disp[3] = {dx, dy, dz};
@@ -997,8 +1357,67 @@ void DmkTree::update_shift(long i, double dx, double dy, double dz) {
   diff_cached_ = false;
 }
 
+// One cooperative launch per kMcChunk moves on every SM (k_mc). The grid is
+// the SM count, which the occupancy query confirms can be co-resident; the
+// cooperative launch refuses to start otherwise, so the grid barriers inside
+// cannot wait on a block that never runs.
+void DmkTree::mc_run_persistent(int n_moves, const int* d_idx, const double* d_disp, const double* d_u, double beta,
+                                double* d_dE, int* d_acc) {
+  DevTree& D = dev_;
+  const size_t smem = tables_smem(D, D.max_depth, 2);
+  const McKernel kern = mc_kernel(D.n_poly);
+  if (mc_grid_ == 0) {
+    int dev = 0, sms = 0, coop = 0;
+    PDMK_CUDA(cudaGetDevice(&dev));
+    PDMK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    PDMK_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) throw CudaError("device does not support cooperative launches");
+    static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
+    const int slot = (D.n_poly - 7) / 6;
+    if (smem > smem_set[slot]) {
+      PDMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      smem_set[slot] = smem;
+    }
+    int per_sm = 0;
+    PDMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, MC_T, smem));
+    if (per_sm < 1) throw CudaError("persistent Metropolis kernel does not fit on one SM");
+    mc_partials_ = static_cast<double*>(alloc(sizeof(double) * 8 * size_t(sms)));
+    mc_sync_ = static_cast<unsigned int*>(alloc(64));
+    mc_grid_ = sms;
+  }
+  const double pi = 3.14159265358979323846;
+  for (int m0 = 0; m0 < n_moves; m0 += kMcChunk) {
+    const int cnt = std::min(kMcChunk, n_moves - m0);
+    PDMK_CUDA(cudaMemsetAsync(mc_sync_, 0, 64, st_));
+    McArgs a{};
+    a.idx = d_idx + m0;
+    a.disp = d_disp + 3 * size_t(m0);
+    a.u = d_u + m0;
+    a.beta = beta;
+    a.n_moves = cnt;
+    a.dE_out = d_dE ? d_dE + m0 : nullptr;
+    a.acc_out = d_acc ? d_acc + m0 : nullptr;
+    a.c_window = std::pow(D.delta_k[0], 3) / std::pow(2 * pi, 3);
+    a.partials = mc_partials_;
+    a.arrivals = mc_sync_;
+    a.spin_limit = 1LL << 21;  // about a second of polling
+    void* args[] = {&D, &a};
+    time_begin(2);
+    PDMK_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kern), dim3(unsigned(mc_grid_)),
+                                          dim3(unsigned(MC_T)), args, smem, st_));
+    PDMK_LAUNCH_CHECK();
+    time_end(2);
+  }
+}
+
 void DmkTree::mc_run_device(int n_moves, const int* d_idx, const double* d_disp, const double* d_u, double beta,
                             double* d_dE, int* d_acc) {
+  if (mc_mode_ == 0) {
+    if (n_moves > 0) mc_run_persistent(n_moves, d_idx, d_disp, d_u, beta, d_dE, d_acc);
+    last_valid_ = false;
+    diff_cached_ = false;
+    return;
+  }
   ensure_move_resources();
   int m = 0;
   // whole batches run as one captured graph each; with timing on, one batch

@@ -121,7 +121,7 @@ struct DevTree {
   Proposal* prop;
   Receiver* recv;  // [MAX_RECV]
   int* err;  // device error word (nonzero: pool overflow etc.)
-  unsigned long long* work;  // [0] accepted moves, [1] update bytes (read + write)
+  unsigned long long* work;  // [0] accepted moves, [1] update bytes (read + write), [2] dE bytes (persistent kernel)
 };
 
 // per-level geometry, computed rather than indexed: box side L 2^-l, the
@@ -185,6 +185,10 @@ class DmkTree {
   // sequential Metropolis over device-resident proposals; no host sync
   void mc_run_device(int n_moves, const int* d_idx, const double* d_disp, const double* d_u, double beta,
                      double* d_dE, int* d_acc);
+  // Metropolis sequence mode: 0 one persistent cooperative launch (default),
+  // 1 CUDA graphs of kGraphMoves (shift, update) launch pairs
+  void set_mc_mode(int mode) { mc_mode_ = mode; }
+  int mc_mode() const { return mc_mode_; }
   // batched energy shifts of many candidates against the current state
   void shift_batch_device(int m, const int* d_idx, const double* d_disp, double* d_dE);
   // the same batch through one fixed static device buffer: no device
@@ -276,6 +280,13 @@ class DmkTree {
   int shift_grid_ = 0;
   // captured Metropolis batches (plain, and with per-update timing events)
   static constexpr int kGraphMoves = 128;
+  static constexpr int kMcChunk = 1 << 16;  // moves per persistent launch
+  int mc_mode_ = 0;
+  int mc_grid_ = 0;
+  double* mc_partials_ = nullptr;
+  unsigned int* mc_sync_ = nullptr;
+  void mc_run_persistent(int n_moves, const int* d_idx, const double* d_disp, const double* d_u, double beta,
+                         double* d_dE, int* d_acc);
   static constexpr int kTimedEvery = 8;
   long timed_batches_ = 0;
   cudaGraphExec_t mc_graph_[2] = {nullptr, nullptr};

@@ -21,6 +21,8 @@ import numpy as np
 DIRECT = 1
 PROXY = 2
 STATIC_MAX_MOVES = 4096  # HPDMK_STATIC_MAX_MOVES in include/hpdmk.h
+MC_PERSISTENT = 0  # HPDMK_MC_PERSISTENT
+MC_GRAPH = 1  # HPDMK_MC_GRAPH
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -89,6 +91,8 @@ def load_library():
                                          ctypes.c_void_p, ctypes.c_void_p]
     L.hpdmk_get_stream.restype = ctypes.c_int
     L.hpdmk_get_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    L.hpdmk_set_mc_mode.restype = ctypes.c_int
+    L.hpdmk_set_mc_mode.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.hpdmk_set_timing.restype = ctypes.c_int
     L.hpdmk_set_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.hpdmk_get_timing.restype = ctypes.c_int
@@ -291,15 +295,19 @@ class HPDMKPtTree:
     def set_timing(self, on: bool):
         _check(load_library().hpdmk_set_timing(self._h, 1 if on else 0))
 
+    def set_mc_mode(self, mode):
+        """MC_PERSISTENT (one cooperative launch, default) or MC_GRAPH (graphs of launch pairs)."""
+        _check(load_library().hpdmk_set_mc_mode(self._h, int(mode)))
+
     def get_timing(self, reset=False):
-        """{class: (total ms, launches)} for shift, update, commit and nudft kernels."""
+        """{class: (total ms, launches)} for shift, update, persistent Metropolis and nudft kernels."""
         o = np.zeros(8)
         _check(load_library().hpdmk_get_timing(self._h, _p(o), 1 if reset else 0))
-        return {k: (o[2 * c], int(o[2 * c + 1])) for c, k in enumerate(("shift", "update", "commit", "nudft"))}
+        return {k: (o[2 * c], int(o[2 * c + 1])) for c, k in enumerate(("shift", "update", "mc", "nudft"))}
 
     def update_work(self):
-        """(accepted moves, algorithmic update bytes) of the last MC batch."""
-        o = np.zeros(2)
+        """(accepted moves, algorithmic update bytes, dE bytes of the persistent kernel) of the last MC batch."""
+        o = np.zeros(3)
         _check(load_library().hpdmk_get_update_bytes(self._h, _p(o)))
         return o
 

@@ -131,7 +131,7 @@ def test_overflow_pool_and_repack():
         assert abs(g.eval_shift_energy(i, *d) - o.eval_shift_energy(i, *d)) <= ABS_DE
 
 
-def test_batch_and_metropolis():
+def test_batch():
     g, o, r, q = pair("uniform", 3000, 14.4, 12, 9, seed=9)
     for t in (g, o):
         t.form_outgoing_pw()
@@ -143,24 +143,52 @@ def test_batch_and_metropolis():
     dg = g.eval_shift_energy_batch(idx, disp)
     do = np.array([o.eval_shift_energy(i, *d) for i, d in zip(idx, disp)])
     assert np.abs(dg - do).max() <= ABS_DE
-    # sequential Metropolis: the oracle replays the same proposals; 300 moves
-    # run as two captured 128-move graphs plus 44 direct launches
+
+
+METROPOLIS_CASES = [
+    ("uniform", 3000, 14.4, 12, 9, 8),
+    ("clustered", 4000, 20.0, 10, 6, 0),   # no slack: arrivals go to the overflow pool
+    ("uniform", 1500, 10.0, 10, 12, 2),
+    ("reference", 1000, 20.0, 10, 3, 4),
+]
+
+
+@pytest.mark.parametrize("mode", [P.MC_PERSISTENT, P.MC_GRAPH])
+@pytest.mark.parametrize("case", METROPOLIS_CASES)
+def test_metropolis(mode, case):
+    # sequential Metropolis: the oracle replays the same proposals. The graph
+    # mode runs 300 moves as two captured 128-move graphs plus 44 direct
+    # launch pairs; the persistent mode as one cooperative launch.
+    kind, n, L, npl, digits, slack = case
+    g, o, r, q = pair(kind, n, L, npl, digits, slack=slack, seed=9)
+    g.set_mc_mode(mode)
+    for t in (g, o):
+        t.form_outgoing_pw()
+        t.form_incoming_pw()
+    rng = np.random.default_rng(2)
     m = 300
-    idx = rng.integers(0, 3000, m)
+    idx = rng.integers(0, n, m)
     disp = rng.uniform(-0.5, 0.5, (m, 3))
     u = rng.uniform(0, 1, m)
     beta = 1.0
     dEg, accg = g.mc_run(idx, disp, u, beta)
     for c in range(m):
         de = o.eval_shift_energy(idx[c], *disp[c])
-        assert abs(de - dEg[c]) <= ABS_DE, c
+        assert abs(de - dEg[c]) <= ABS_DE * max(1.0, abs(de)), c
         acc = u[c] < np.exp(-beta * de)
         assert abs(u[c] - np.exp(-beta * de)) < 1e-9 or acc == bool(accg[c])
         if accg[c]:
             o.update_shift(idx[c], *disp[c])
+    assert accg.sum() > 0
     np.testing.assert_array_equal(g.positions(), o.positions())
     pg, po = g.eval_energy_parts(), o.eval_energy_parts()
     assert np.all(np.abs(pg - po) <= REL_E * abs(po.sum()))
+    # a second run continues from the updated state
+    idx = rng.integers(0, n, 40)
+    disp = rng.uniform(-0.5, 0.5, (40, 3))
+    dg = g.eval_shift_energy_batch(idx, disp)
+    do = np.array([o.eval_shift_energy(i, *d) for i, d in zip(idx, disp)])
+    assert np.abs(dg - do).max() <= ABS_DE * max(1.0, np.abs(do).max())
 
 
 @pytest.mark.parametrize("digits", [3, 6, 9, 12])
