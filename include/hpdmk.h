@@ -135,10 +135,12 @@ int hpdmk_eval_shift_energy_batch(hpdmk_tree tree, int m, const long *i, const d
  * the call allocates no device memory: its block partials, completion counter,
  * proposal record, phase tables and staged inputs/outputs live in one fixed
  * static device buffer (about 250 KB per device, found once per device). For
- * callers that must not allocate once the tree exists.
+ * callers that may not allocate device memory once the tree exists: a process
+ * that budgets its device memory up front, or one whose memory is handed out
+ * by another framework's pool that it must not grow or bypass.
  * Limits: m <= HPDMK_STATIC_MAX_MOVES; larger m returns HPDMK_ERR_BAD_INPUT
- * with a message and does no work. The buffer's completion counter must be
- * zero at a launch: it is zero at load and every launch leaves it at zero.
+ * with a message and does no work. The buffer keeps the last call's contents;
+ * its completion counter must start at zero, and each call clears it.
  * Calls that overlap in time on one device share the buffer and race: make
  * them one after another. Make the first call on each device before any
  * stream capture starts, since it looks up the buffer's address. */

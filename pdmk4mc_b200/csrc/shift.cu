@@ -1462,8 +1462,8 @@ void DmkTree::shift_batch_device(int m, const int* d_idx, const double* d_disp, 
 // host thread that must not enter the allocator between steps): the block
 // partials, completion counter, proposal record, phase tables and the staged
 // inputs/outputs all live in g_static_scratch, whose address is looked up once
-// per device. The completion counter must be zero when a launch starts: the
-// buffer is zero at module load and every launch's last block sets it back.
+// per device. The completion counter must be zero when a launch starts: each
+// call clears it, and every launch's last block sets it back to zero.
 // Calls that overlap in time on one device (two host threads, two trees on
 // different streams) share the buffer and race; serialise them.
 namespace {
@@ -1526,6 +1526,9 @@ void DmkTree::shift_batch_static(int m, const long* h_idx, const double* h_disp,
     PDMK_CUDA(cudaMemcpyAsync(s_idx + c0, chunk, sizeof(int) * nc, cudaMemcpyHostToDevice, st_));
   }
   PDMK_CUDA(cudaMemcpyAsync(s_disp, h_disp, sizeof(double) * 3 * m, cudaMemcpyHostToDevice, st_));
+  // the buffer keeps what the last call left; the completion counter must
+  // start at zero, so clear it (a launch that was cut short leaves it set)
+  PDMK_CUDA(cudaMemsetAsync(base + kOffCounter, 0, sizeof(unsigned int), st_));
   const double pi = 3.14159265358979323846;
   ShiftArgs a{};
   a.idx = s_idx;

@@ -1,5 +1,7 @@
 """The static-buffer candidate batch (hpdmk_eval_shift_energy_batch_static, no
-reference counterpart) against the allocating hpdmk_eval_shift_energy_batch:
+reference counterpart; it serves callers that may not allocate device memory
+after the tree exists, such as a process with a fixed device-memory budget)
+against the allocating hpdmk_eval_shift_energy_batch:
 same kernel, same deterministic reductions, so the results must be identical,
 on consecutive calls and across trees that share the one static buffer. Kept
 in a file that sorts last so it also runs after every other GPU test."""
