@@ -43,15 +43,6 @@ __device__ inline double center_of(double L, int l, int X) {
   return L * (double(X) * scale + 0.5 * scale);
 }
 
-__device__ inline void node_center(const DevTree& T, int node, double* c, int* X) {
-  const uint64_t p = T.node_prefix[node];
-  const int l = T.node_level[node];
-  X[0] = int(compact3(p));
-  X[1] = int(compact3(p >> 1));
-  X[2] = int(compact3(p >> 2));
-  for (int d = 0; d < 3; ++d) c[d] = center_of(T.L, l, X[d]);
-}
-
 __device__ inline int periodic_shift_d(double xi, double xj, double L, double bi, double bj) {
   if (xi < bi && xj > (L - bj)) return 1;
   if (xi > (L - bi) && xj < bj) return -1;
@@ -82,26 +73,6 @@ __device__ inline void alloc_tables(double2* sm, const DevTree& T, Tables& tb) {
   tb.lev = Tables::Levels{sm, 2 * T.n_window + 1, 2 * T.n_diff + 1};
 }
 
-__device__ inline void axis_table(double xr, double dk, int M, int X, int n, int cnt, double scale, double2* dst,
-                                  int part, int nparts) {
-  // entries m = -n .. -n+cnt-1, split in nparts contiguous pieces
-  int per = (cnt + nparts - 1) / nparts;
-  int a = part * per, b = min(cnt, a + per);
-  if (a >= b) return;
-  int m0 = -n + a;
-  double th = dk * xr;
-  double s, c;
-  sincos(-double(m0) * th, &s, &c);
-  double2 v = make_double2(c * scale, s * scale);
-  sincos(-th, &s, &c);
-  const double2 step = make_double2(c, s);
-  const int dec = M * (2 * X + 1);
-  for (int t = a; t < b; ++t) {
-    dst[t] = cmul(v, root6(-dec * (m0 + t - a)));
-    v = cmul(v, step);
-  }
-}
-
 struct Header {
   int i_orig, slot;
   double q;
@@ -112,27 +83,52 @@ struct Header {
   int Xo[MAXLV][3], Xt[MAXLV][3];  // integer box coordinates along each path
 };
 
-// Tables of one point on its path for levels 2..lmax; block-cooperative.
-// Box-centred phases with the exact decentring root of unity per axis.
+// Tables of one point on its path for levels 2..lmax, one entry per thread
+// (threads t0, t0 + nthr, ...): e^{-i m dk_l (x - c_l)} with the box-centred
+// phase and the exact decentring root of unity, times q on the z axis. Every
+// entry is its own sincos, so the table costs one sincos latency instead of
+// a chain of recurrence steps.
 __device__ void build_tables(const DevTree& T, const double* x, double q, const int (*X)[3], int lmax,
-                             const Tables& tb) {
-  const int NP = 4;  // pieces per axis
+                             const Tables& tb, int t0, int nthr) {
+  const int nw = T.n_window, nd = T.n_diff;
+  const int root_n = 2 * (2 * nw + 1) + (nw + 1);
+  const int lev_n = 2 * (2 * nd + 1) + (nd + 1);
   const int nlev = lmax >= 2 ? lmax - 1 : 0;
-  const int ntask = (1 + nlev) * 3 * NP;
-  for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
-    int part = t % NP, axis = (t / NP) % 3, slot = t / (3 * NP);
-    if (slot == 0) {
-      int n = T.n_window;
-      int cnt = axis == 2 ? n + 1 : 2 * n + 1;
-      axis_table(x[axis] - 0.5 * T.L, T.delta_k[0], 3, 0, n, cnt, axis == 2 ? q : 1.0, tb.root[axis], part, NP);
+  const int total = root_n + nlev * lev_n;
+  for (int e = t0; e < total; e += nthr) {
+    int slot, rem;
+    if (e < root_n) {
+      slot = 0;
+      rem = e;
     } else {
-      int l = slot + 1;
-      int Xa = X[l][axis];
-      int n = T.n_diff;
-      int cnt = axis == 2 ? n + 1 : 2 * n + 1;
-      axis_table(x[axis] - center_of(T.L, l, Xa), level_dk(T, l), 1, Xa, n, cnt, axis == 2 ? q : 1.0,
-                 tb.lev[l][axis], part, NP);
+      slot = 1 + (e - root_n) / lev_n;
+      rem = (e - root_n) % lev_n;
     }
+    const int n = slot == 0 ? nw : nd;
+    const int w = 2 * n + 1;
+    const int axis = rem < w ? 0 : (rem < 2 * w ? 1 : 2);
+    const int t = rem - axis * w;
+    const int m = t - n;
+    double xr, dk;
+    int dec;
+    double2* dst;
+    if (slot == 0) {
+      xr = x[axis] - 0.5 * T.L;
+      dk = T.delta_k[0];
+      dec = 3;
+      dst = tb.root[axis];
+    } else {
+      const int l = slot + 1, Xa = X[l][axis];
+      xr = x[axis] - center_of(T.L, l, Xa);
+      dk = level_dk(T, l);
+      dec = 2 * Xa + 1;
+      dst = tb.lev[l][axis];
+    }
+    const double th = dk * xr;
+    double sn, cs;
+    sincos(-double(m) * th, &sn, &cs);
+    const double sc = axis == 2 ? q : 1.0;
+    dst[t] = cmul(make_double2(cs * sc, sn * sc), root6(-dec * m));
   }
 }
 
@@ -156,10 +152,10 @@ __device__ inline V ldm(const V* p) {
 }
 
 template <bool CG = false>
-__device__ void resolve(const DevTree& T, int i, const double* disp, Header& h) {
+__device__ void resolve(const DevTree& T, int i, const double* disp, Header& h, int s_known = -1) {
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
-    const int s = ldm<CG>(T.orig_slot + i);
+    const int s = s_known >= 0 ? s_known : ldm<CG>(T.orig_slot + i);
     double xo[3], q;
     if (s < T.n_slots) {
       xo[0] = ldm<CG>(T.sx + s);
@@ -510,8 +506,8 @@ __global__ void __launch_bounds__(SH_T) k_shift(DevTree T, ShiftArgs a) {
     Tables to, oo;
     alloc_tables(sm2, T, oo);
     alloc_tables(sm2 + per, T, to);
-    build_tables(T, h.xo, h.q, h.Xo, uo, oo);
-    build_tables(T, h.xt, h.q, h.Xt, ut, to);
+    build_tables(T, h.xo, h.q, h.Xo, uo, oo, threadIdx.x, blockDim.x);
+    build_tables(T, h.xt, h.q, h.Xt, ut, to, threadIdx.x, blockDim.x);
     __syncthreads();
     if (blockIdx.x == 0) {
       // publish the tables for k_update
@@ -629,14 +625,6 @@ constexpr int UPD_UNROLL = 8;
 
 __device__ void commit_move(const DevTree& T, const Proposal& P);
 
-__device__ inline double2 image_phase(double2 p, const signed char* f, int ix, int iy, int iz, int n, int two_l) {
-  if (f[0] | f[1] | f[2]) {
-    const int sg = ((ix - n) * f[0] + (iy - n) * f[1] + (iz - n) * f[2]) * two_l;
-    p = cmul(p, root6(-2 * (sg % 3)));
-  }
-  return p;
-}
-
 __global__ void __launch_bounds__(UPD_T) k_update(DevTree T, const double2* __restrict__ ptab, long ptab_per) {
   __shared__ Receiver rs[MAX_RECV];
   __shared__ int s_acc, s_nr;
@@ -669,6 +657,7 @@ __global__ void __launch_bounds__(UPD_T) k_update(DevTree T, const double2* __re
   if (k >= T.H) return;
   const int n = T.n_diff, d = T.dd;
   const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
+  const int a0 = ((ix - n) % 3 + 3) % 3, a1 = ((iy - n) % 3 + 3) % 3, a2 = ((iz - n) % 3 + 3) % 3;
   int r = 0;
   const int nloc = r1 - r0;
   while (r < nloc) {
@@ -676,8 +665,10 @@ __global__ void __launch_bounds__(UPD_T) k_update(DevTree T, const double2* __re
     const int l = rs[r].level;
     int re = r + 1;
     while (re < nloc && rs[re].level == l) ++re;
-    const double2 pt = cmul(tt.lev[l][2][iz], cmul(tt.lev[l][1][iy], tt.lev[l][0][ix]));
-    const double2 po = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
+    const double2 pt0 = cmul(tt.lev[l][2][iz], cmul(tt.lev[l][1][iy], tt.lev[l][0][ix]));
+    const double2 po0 = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
+    const double2 pt1 = cmul(pt0, root6(-2)), pt2 = cmul(pt0, root6(-4));
+    const double2 po1 = cmul(po0, root6(-2)), po2 = cmul(po0, root6(-4));
     const int two_l = (l & 1) ? 2 : 1;
     for (; r < re; r += UPD_UNROLL) {
       double2 v[UPD_UNROLL];
@@ -694,9 +685,12 @@ __global__ void __launch_bounds__(UPD_T) k_update(DevTree T, const double2* __re
       for (int u = 0; u < UPD_UNROLL; ++u) {
         if (r + u < re) {
           const Receiver& R = rs[r + u];
+          // image phase: a cube root of unity, w^-e with e in [-12, 12] mod 3
+          const int et = ((a0 * R.ft[0] + a1 * R.ft[1] + a2 * R.ft[2]) * two_l + 12) % 3;
+          const int eo = ((a0 * R.fo[0] + a1 * R.fo[1] + a2 * R.fo[2]) * two_l + 12) % 3;
           double2 del = make_double2(0.0, 0.0);
-          if (R.has_t) del = image_phase(pt, R.ft, ix, iy, iz, n, two_l);
-          if (R.has_o) del = csub(del, image_phase(po, R.fo, ix, iy, iz, n, two_l));
+          if (R.has_t) del = et == 0 ? pt0 : (et == 1 ? pt1 : pt2);
+          if (R.has_o) del = csub(del, eo == 0 ? po0 : (eo == 1 ? po1 : po2));
           if (R.is_out) T.out[off[u]] = cadd(v[u], del);
           else T.inc[off[u]] = make_double2(v[u].x + del.x, v[u].y - del.y);
         }
@@ -706,81 +700,83 @@ __global__ void __launch_bounds__(UPD_T) k_update(DevTree T, const double2* __re
   }
 }
 
-// particle membership and position (exact on every level); one thread
+// particle membership and position (exact on every level); one thread. The
+// independent loads are issued together and the per-level counts change by
+// atomic adds that need no reply, so the thread waits on few round trips.
 __device__ void commit_move(const DevTree& T, const Proposal& P) {
   if (!P.accepted) return;
   const int leafA = P.path_o[P.depth_o - 1];
   const int leafB = P.path_t[P.depth_t - 1];
   const int i = P.i_orig;
-  int s = P.slot;
+  const int s = P.slot;
+  const double xt0 = P.xt[0], xt1 = P.xt[1], xt2 = P.xt[2], q = P.q;
   if (leafA == leafB) {
     if (s < T.n_slots) {
-      T.sx[s] = P.xt[0];
-      T.sy[s] = P.xt[1];
-      T.sz[s] = P.xt[2];
+      T.sx[s] = xt0;
+      T.sy[s] = xt1;
+      T.sz[s] = xt2;
     } else {
-      int p = s - T.n_slots;
-      T.px[p] = P.xt[0];
-      T.py[p] = P.xt[1];
-      T.pz[p] = P.xt[2];
+      const int p = s - T.n_slots;
+      T.px[p] = xt0;
+      T.py[p] = xt1;
+      T.pz[p] = xt2;
     }
     return;
   }
+  const int cA = T.leaf_count[leafA], begA = T.node_begin[leafA];
+  const int cB = T.leaf_count[leafB], begB = T.node_begin[leafB], endB = T.node_end[leafB];
+  const int pn = *T.pool_n;
   // remove from the origin leaf (swap with its last particle) or the pool
   if (s < T.n_slots) {
-    int cA = T.leaf_count[leafA];
-    int last = T.node_begin[leafA] + cA - 1;
+    const int last = begA + cA - 1;
+    const int ol = T.s_orig[last];
+    const double lx = T.sx[last], ly = T.sy[last], lz = T.sz[last], lq = T.sq[last];
+    const uint64_t pfx = T.node_prefix[leafA];
+    const int lvl = T.node_level[leafA];
     if (s != last) {
-      int ol = T.s_orig[last];
-      T.sx[s] = T.sx[last];
-      T.sy[s] = T.sy[last];
-      T.sz[s] = T.sz[last];
-      T.sq[s] = T.sq[last];
+      T.sx[s] = lx;
+      T.sy[s] = ly;
+      T.sz[s] = lz;
+      T.sq[s] = lq;
       T.s_orig[s] = ol;
       T.orig_slot[ol] = s;
     }
-    double c[3];
-    int X[3];
-    node_center(T, leafA, c, X);
-    T.sx[last] = c[0];
-    T.sy[last] = c[1];
-    T.sz[last] = c[2];
+    // a freed slot holds a zero charge at its leaf's centre
+    T.sx[last] = center_of(T.L, lvl, int(compact3(pfx)));
+    T.sy[last] = center_of(T.L, lvl, int(compact3(pfx >> 1)));
+    T.sz[last] = center_of(T.L, lvl, int(compact3(pfx >> 2)));
     T.sq[last] = 0.0;
     T.s_orig[last] = -1;
     T.leaf_count[leafA] = cA - 1;
   } else {
-    int p = s - T.n_slots;
+    const int p = s - T.n_slots;
     T.p_orig[p] = -1;
     T.pq[p] = 0.0;
   }
   // insert into the target leaf, or park in the pool when it is full
-  int cB = T.leaf_count[leafB];
-  int slot = T.node_begin[leafB] + cB;
-  if (slot < T.node_end[leafB]) {
-    T.sx[slot] = P.xt[0];
-    T.sy[slot] = P.xt[1];
-    T.sz[slot] = P.xt[2];
-    T.sq[slot] = P.q;
+  const int slot = begB + cB;
+  if (slot < endB) {
+    T.sx[slot] = xt0;
+    T.sy[slot] = xt1;
+    T.sz[slot] = xt2;
+    T.sq[slot] = q;
     T.s_orig[slot] = i;
     T.orig_slot[i] = slot;
     T.leaf_count[leafB] = cB + 1;
+  } else if (pn < T.pool_cap) {
+    T.px[pn] = xt0;
+    T.py[pn] = xt1;
+    T.pz[pn] = xt2;
+    T.pq[pn] = q;
+    T.p_orig[pn] = i;
+    T.p_leaf[pn] = leafB;
+    T.orig_slot[i] = T.n_slots + pn;
+    *T.pool_n = pn + 1;
   } else {
-    int p = *T.pool_n;
-    if (p < T.pool_cap) {
-      T.px[p] = P.xt[0];
-      T.py[p] = P.xt[1];
-      T.pz[p] = P.xt[2];
-      T.pq[p] = P.q;
-      T.p_orig[p] = i;
-      T.p_leaf[p] = leafB;
-      T.orig_slot[i] = T.n_slots + p;
-      *T.pool_n = p + 1;
-    } else {
-      *T.err = 1;  // pool exhausted: the host repacks and reports
-    }
+    *T.err = 1;  // pool exhausted: the host repacks and reports
   }
-  for (int l = 0; l < P.depth_o; ++l) T.node_count[P.path_o[l]] -= 1;
-  for (int l = 0; l < P.depth_t; ++l) T.node_count[P.path_t[l]] += 1;
+  for (int l = 0; l < P.depth_o; ++l) atomicAdd(T.node_count + P.path_o[l], -1);
+  for (int l = 0; l < P.depth_t; ++l) atomicAdd(T.node_count + P.path_t[l], 1);
 }
 
 
@@ -826,8 +822,9 @@ __device__ bool mc_barrier(const DevTree& T, const McArgs& a, unsigned& nbar) {
   if (threadIdx.x == 0) {
     ++nbar;
     const unsigned target = nbar * gridDim.x;
-    __threadfence();
-    atomicAdd(a.arrivals, 1u);
+    // the release orders this block's writes (made visible to this thread by
+    // the __syncthreads above) before the arrival; no reply is awaited
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(a.arrivals) : "memory");
     int ok = 1;
     for (long long it = 0;; ++it) {
       if (ld_acquire(a.arrivals) >= target) break;
@@ -895,7 +892,12 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
   __shared__ Receiver rs[MAX_RECV];
   __shared__ Proposal P;
   __shared__ int s_acc;
+  __shared__ int s_rounds[9];  // grid-stride rounds of H*g update units
   const ResidualPoly<NP> poly(T);
+  if (threadIdx.x >= 1 && threadIdx.x <= 8) {
+    const long units = long(T.H) * threadIdx.x, gs = long(gridDim.x) * blockDim.x;
+    s_rounds[threadIdx.x] = int((units + gs - 1) / gs);
+  }
   if (threadIdx.x >= 2 && threadIdx.x < MAXLV + 2) {
     const double dk = level_dk(T, threadIdx.x);
     c_level[threadIdx.x] = dk * dk * dk / (8.0 * 3.14159265358979323846 * 3.14159265358979323846 *
@@ -904,9 +906,21 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
   const int G = gridDim.x;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gstride = G * blockDim.x;
   unsigned nbar = 0;
+  // warp 0 runs one proposal ahead: the next index is loaded at the top of a
+  // move and its slot after the sums, so the next resolve starts from them
+  // unless the accepted move changed that slot
+  int i_cur = threadIdx.x < 32 ? a.idx[0] : 0, s_hint = -1;
   for (int m = 0; m < a.n_moves; ++m) {
-    resolve<true>(T, a.idx[m], a.disp + 3 * m, h);
+    const int i_next = (threadIdx.x < 32 && m + 1 < a.n_moves) ? a.idx[m + 1] : 0;
+    resolve<true>(T, i_cur, a.disp + 3 * m, h, s_hint);
     const int lo_max = h.depth_o - 2, lt_max = h.depth_t - 2;
+    // the incoming rows of both paths go to L2 while the tables are built
+    for (int k = gt; k < T.H; k += gstride) {
+      for (int l = 2; l <= lo_max; ++l)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(T.inc + size_t(h.path_o[l] - T.pw_base) * T.H + k));
+      for (int l = 2; l <= lt_max; ++l)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(T.inc + size_t(h.path_t[l] - T.pw_base) * T.H + k));
+    }
     const int uo = min(h.depth_o - 1, T.pw_hi), ut = min(h.depth_t - 1, T.pw_hi);
     const int per = 3 * (2 * T.n_window + 1) + max(max(uo, ut) - 1, 0) * 3 * (2 * T.n_diff + 1);
     Tables to, oo;
@@ -918,27 +932,9 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
       const int lv = (p == 0 ? h.depth_t : h.depth_o) - 1;
       res_meta(T, p == 0 ? h.path_t[lv] : h.path_o[lv], lv, p == 0 ? h.Xt[lv] : h.Xo[lv], src, meta[p]);
     } else {
-      const int NPT = 4, nthr = blockDim.x - 72, t = threadIdx.x - 72;
-      for (int path = 0; path < 2; ++path) {
-        const int lmax = path == 0 ? uo : ut;
-        const int nlev = lmax >= 2 ? lmax - 1 : 0;
-        const int ntask = (1 + nlev) * 3 * NPT;
-        const double* x = path == 0 ? h.xo : h.xt;
-        const int(*X)[3] = path == 0 ? h.Xo : h.Xt;
-        const Tables& tb = path == 0 ? oo : to;
-        for (int k = t; k < ntask; k += nthr) {
-          const int part = k % NPT, axis = (k / NPT) % 3, slot = k / (3 * NPT);
-          if (slot == 0) {
-            const int n = T.n_window, cnt = axis == 2 ? n + 1 : 2 * n + 1;
-            axis_table(x[axis] - 0.5 * T.L, T.delta_k[0], 3, 0, n, cnt, axis == 2 ? h.q : 1.0, tb.root[axis], part,
-                       NPT);
-          } else {
-            const int l = slot + 1, Xa = X[l][axis], n = T.n_diff, cnt = axis == 2 ? n + 1 : 2 * n + 1;
-            axis_table(x[axis] - center_of(T.L, l, Xa), level_dk(T, l), 1, Xa, n, cnt, axis == 2 ? h.q : 1.0,
-                       tb.lev[l][axis], part, NPT);
-          }
-        }
-      }
+      const int nthr = blockDim.x - 72, t = threadIdx.x - 72;
+      build_tables(T, h.xo, h.q, h.Xo, uo, oo, t, nthr);
+      build_tables(T, h.xt, h.q, h.Xt, ut, to, t, nthr);
     }
     __syncthreads();
     if (threadIdx.x < 2) {
@@ -1019,6 +1015,7 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
       acc[2] *= h.q;
       acc[3] *= h.q;
     }
+    const int s_next = threadIdx.x < 32 ? __ldcg(T.orig_slot + i_next) : 0;
     block_sum4(acc, red);
     double* part = a.partials + size_t(m & 1) * 4 * G;
     if (threadIdx.x == 0)
@@ -1047,9 +1044,37 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
       }
     }
     __syncthreads();
+    if (threadIdx.x < 32) {
+      // the next particle's slot is stale when an accepted move changed leaves
+      // (its own slot and the slot of the particle swapped into its place) or
+      // moved that very particle
+      const bool stale = s_acc && (h.path_o[h.depth_o - 1] != h.path_t[h.depth_t - 1] || i_next == h.i_orig);
+      s_hint = stale ? -1 : s_next;
+      if (!stale && threadIdx.x == 0 && s_next < T.n_slots) {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(T.sx + s_next));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(T.sy + s_next));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(T.sz + s_next));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(T.sq + s_next));
+      }
+      i_cur = i_next;
+    }
     if (!s_acc) continue;
     // accept-and-update (src/tree.cpp:447-597)
     const int nr = build_receivers(T, h, rs);
+    // receiver groups per mode: the g that minimises grid-stride rounds of
+    // the H*g units times receivers per group
+    int ng = 1;
+    {
+      int best = 1 << 30;
+#pragma unroll
+      for (int g = 1; g <= 8; ++g) {
+        const int cost = s_rounds[g] * ((nr + g - 1) / g);
+        if (cost < best) {
+          best = cost;
+          ng = g;
+        }
+      }
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       P.i_orig = h.i_orig;
       P.slot = h.slot;
@@ -1072,28 +1097,33 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
       commit_move(T, P);
     }
     {
-      const int Hk = ((max(T.H, T.Hw) + 31) / 32) * 32;
-      const int ng = max(1, min(8, gstride / Hk));
+      // root window: out_root += t - o
+      for (int k = gt; k < T.Hw; k += gstride) {
+        const double2 t = phase_at(to.root, k, T.dw), o = phase_at(oo.root, k, T.dw);
+        double2 g = __ldcg(T.out_root + k);
+        g = cadd(g, t);
+        g = csub(g, o);
+        T.out_root[k] = g;
+      }
+      // units (mode k, receiver group): a thread walks its group's receivers
+      // in level runs. A periodic image multiplies a single-particle phase by
+      // a cube root of unity w^-e, e = (k - n).f * 2^l mod 3, so each run
+      // precomputes p, p w^-1, p w^-2 and a receiver only picks one.
       const int n = T.n_diff, d = T.dd;
-      for (int item = gt; item < Hk * ng; item += gstride) {
-        const int k = item % Hk, rg = item / Hk;
-        if (rg == 0 && k < T.Hw) {
-          const double2 t = phase_at(to.root, k, T.dw), o = phase_at(oo.root, k, T.dw);
-          double2 g = __ldcg(T.out_root + k);
-          g = cadd(g, t);
-          g = csub(g, o);
-          T.out_root[k] = g;
-        }
-        if (k >= T.H) continue;
+      for (int u = gt; u < T.H * ng; u += gstride) {
+        const int k = u % T.H, rg = u / T.H;
         const int r0 = (rg * nr) / ng, r1 = ((rg + 1) * nr) / ng;
         const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
+        const int a0 = ((ix - n) % 3 + 3) % 3, a1 = ((iy - n) % 3 + 3) % 3, a2 = ((iz - n) % 3 + 3) % 3;
         int r = r0;
         while (r < r1) {
           const int l = rs[r].level;
           int re = r + 1;
           while (re < r1 && rs[re].level == l) ++re;
-          const double2 pt = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
-          const double2 po = cmul(oo.lev[l][2][iz], cmul(oo.lev[l][1][iy], oo.lev[l][0][ix]));
+          const double2 pt0 = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
+          const double2 po0 = cmul(oo.lev[l][2][iz], cmul(oo.lev[l][1][iy], oo.lev[l][0][ix]));
+          const double2 pt1 = cmul(pt0, root6(-2)), pt2 = cmul(pt0, root6(-4));
+          const double2 po1 = cmul(po0, root6(-2)), po2 = cmul(po0, root6(-4));
           const int two_l = (l & 1) ? 2 : 1;
           for (; r < re; r += UPD_UNROLL) {
             double2 v[UPD_UNROLL];
@@ -1110,9 +1140,12 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
             for (int q = 0; q < UPD_UNROLL; ++q) {
               if (r + q < re) {
                 const Receiver& R = rs[r + q];
+                // the exponent sum lies in [-12, 12]
+                const int et = ((a0 * R.ft[0] + a1 * R.ft[1] + a2 * R.ft[2]) * two_l + 12) % 3;
+                const int eo = ((a0 * R.fo[0] + a1 * R.fo[1] + a2 * R.fo[2]) * two_l + 12) % 3;
                 double2 del = make_double2(0.0, 0.0);
-                if (R.has_t) del = image_phase(pt, R.ft, ix, iy, iz, n, two_l);
-                if (R.has_o) del = csub(del, image_phase(po, R.fo, ix, iy, iz, n, two_l));
+                if (R.has_t) del = et == 0 ? pt0 : (et == 1 ? pt1 : pt2);
+                if (R.has_o) del = csub(del, eo == 0 ? po0 : (eo == 1 ? po1 : po2));
                 if (R.is_out) T.out[off[q]] = cadd(v[q], del);
                 else T.inc[off[q]] = make_double2(v[q].x + del.x, v[q].y - del.y);
               }
