@@ -151,13 +151,26 @@ __device__ inline V ldm(const V* p) {
   else return *p;
 }
 
+// A particle's slot, position and charge loaded ahead of its resolve (s < 0:
+// nothing loaded).
+struct Preload {
+  int s;
+  double x, y, z, q;
+};
+
 template <bool CG = false>
-__device__ void resolve(const DevTree& T, int i, const double* disp, Header& h, int s_known = -1) {
+__device__ void resolve(const DevTree& T, int i, const double* disp, Header& h, const Preload* pre = nullptr) {
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
-    const int s = s_known >= 0 ? s_known : ldm<CG>(T.orig_slot + i);
+    const bool have = pre && pre->s >= 0;
+    const int s = have ? pre->s : ldm<CG>(T.orig_slot + i);
     double xo[3], q;
-    if (s < T.n_slots) {
+    if (have) {
+      xo[0] = pre->x;
+      xo[1] = pre->y;
+      xo[2] = pre->z;
+      q = pre->q;
+    } else if (s < T.n_slots) {
       xo[0] = ldm<CG>(T.sx + s);
       xo[1] = ldm<CG>(T.sy + s);
       xo[2] = ldm<CG>(T.sz + s);
@@ -893,6 +906,7 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
   __shared__ Proposal P;
   __shared__ int s_acc;
   __shared__ int s_rounds[9];  // grid-stride rounds of H*g update units
+  __shared__ int s_pn;         // overflow pool fill
   const ResidualPoly<NP> poly(T);
   if (threadIdx.x >= 1 && threadIdx.x <= 8) {
     const long units = long(T.H) * threadIdx.x, gs = long(gridDim.x) * blockDim.x;
@@ -905,14 +919,26 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
   }
   const int G = gridDim.x;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gstride = G * blockDim.x;
+  // window and root items run from the end of the grid, the difference and
+  // update units from its start, so no block carries both
+  const int gtr = gstride - 1 - gt;
   unsigned nbar = 0;
-  // warp 0 runs one proposal ahead: the next index is loaded at the top of a
-  // move and its slot after the sums, so the next resolve starts from them
-  // unless the accepted move changed that slot
-  int i_cur = threadIdx.x < 32 ? a.idx[0] : 0, s_hint = -1;
+  // warp 0 runs one proposal ahead: the next index and displacement are
+  // loaded at the top of a move, the next slot after the sums and the
+  // particle itself after the decision, so the next resolve starts from them
+  // unless the accepted move changed that slot or particle
+  int i_cur = threadIdx.x < 32 ? a.idx[0] : 0;
+  double d_cur[3] = {0, 0, 0};
+  if (threadIdx.x < 32)
+    for (int c = 0; c < 3; ++c) d_cur[c] = a.disp[c];
+  Preload pre{-1, 0, 0, 0, 0};
   for (int m = 0; m < a.n_moves; ++m) {
-    const int i_next = (threadIdx.x < 32 && m + 1 < a.n_moves) ? a.idx[m + 1] : 0;
-    resolve<true>(T, i_cur, a.disp + 3 * m, h, s_hint);
+    const bool more = threadIdx.x < 32 && m + 1 < a.n_moves;
+    const int i_next = more ? a.idx[m + 1] : 0;
+    double d_next[3] = {0, 0, 0};
+    if (more)
+      for (int c = 0; c < 3; ++c) d_next[c] = a.disp[3 * (m + 1) + c];
+    resolve<true>(T, i_cur, d_cur, h, &pre);
     const int lo_max = h.depth_o - 2, lt_max = h.depth_t - 2;
     // the incoming rows of both paths go to L2 while the tables are built
     for (int k = gt; k < T.H; k += gstride) {
@@ -928,6 +954,7 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
     alloc_tables(sm2 + per, T, to);
     // near-field source lists on threads 0..71, phase tables on the rest
     if (threadIdx.x < 72) {
+      if (threadIdx.x == 0) s_pn = __ldcg(T.pool_n);
       const int p = threadIdx.x / 36, src = threadIdx.x % 36;
       const int lv = (p == 0 ? h.depth_t : h.depth_o) - 1;
       res_meta(T, p == 0 ? h.path_t[lv] : h.path_o[lv], lv, p == 0 ? h.Xt[lv] : h.Xo[lv], src, meta[p]);
@@ -948,8 +975,31 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
     }
     __syncthreads();
     double acc[4] = {0, 0, 0, 0};
+    // near field of the target and the origin (src/energy_shift.cpp:233-302):
+    // the pairs of both paths split evenly over the blocks. The first pair's
+    // source is loaded before the mode sums so the two latencies overlap.
+    const int nt = meta[0].pre[36], no = meta[1].pre[36], np = nt + no;
+    const int e0 = int((long(blockIdx.x) * np) / G), e1 = int((long(blockIdx.x + 1) * np) / G);
+    const double eps = 2.220446049250313e-16;
+    int e = e0 + threadIdx.x;
+    double4 src_first = make_double4(0, 0, 0, 0);
+    int p_first = 0, srci_first = 0;
+    if (e < e1) {
+      p_first = e < nt ? 0 : 1;
+      const ResMeta& M = meta[p_first];
+      const int ee = p_first == 0 ? e : e - nt;
+      int lo = 0, hi = 36;  // largest src with pre[src] <= ee
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (M.pre[mid] <= ee) lo = mid;
+        else hi = mid;
+      }
+      srci_first = lo;
+      const int sl = M.beg[lo] + (ee - M.pre[lo]);
+      src_first = make_double4(__ldcg(T.sx + sl), __ldcg(T.sy + sl), __ldcg(T.sz + sl), __ldcg(T.sq + sl));
+    }
     // window (src/energy_shift.cpp:72-90)
-    for (int k = gt; k < T.Hw; k += gstride) {
+    for (int k = gtr; k < T.Hw; k += gstride) {
       const double2 t = phase_at(to.root, k, T.dw), o = phase_at(oo.root, k, T.dw);
       const double2 g = __ldcg(T.out_root + k);
       const double ar = t.x - o.x, ai = t.y - o.y, br = g.x - o.x, bi = g.y - o.y;
@@ -974,31 +1024,41 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
         acc[1] += s * T.D2[k];
       }
     }
-    // near field of the target and the origin (src/energy_shift.cpp:233-302):
-    // the pairs of both paths split evenly over the blocks
     {
-      const int nt = meta[0].pre[36], no = meta[1].pre[36], np = nt + no;
-      const int e0 = int((long(blockIdx.x) * np) / G), e1 = int((long(blockIdx.x + 1) * np) / G);
-      const double eps = 2.220446049250313e-16;
-      for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        const int p = e < nt ? 0 : 1;
+      for (; e < e1; e += blockDim.x) {
+        int p, srci;
+        double4 v;
+        if (e == e0 + int(threadIdx.x)) {
+          p = p_first;
+          srci = srci_first;
+          v = src_first;
+        } else {
+          p = e < nt ? 0 : 1;
+          const ResMeta& M = meta[p];
+          const int ee = p == 0 ? e : e - nt;
+          int lo = 0, hi = 36;
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (M.pre[mid] <= ee) lo = mid;
+            else hi = mid;
+          }
+          srci = lo;
+          const int sl = M.beg[lo] + (ee - M.pre[lo]);
+          v = make_double4(__ldcg(T.sx + sl), __ldcg(T.sy + sl), __ldcg(T.sz + sl), __ldcg(T.sq + sl));
+        }
         const ResMeta& M = meta[p];
-        const int ee = p == 0 ? e : e - nt;
-        int src = 0;
-        while (ee >= M.pre[src + 1]) ++src;
         const int lv = (p == 0 ? h.depth_t : h.depth_o) - 1;
         const double b = level_box(T, lv);
         const double* x = p == 0 ? h.xt : h.xo;
-        const int s = M.beg[src] + (ee - M.pre[src]);
-        const double dx = x[0] - (__ldcg(T.sx + s) + M.off[src][0]), dy = x[1] - (__ldcg(T.sy + s) + M.off[src][1]),
-                     dz = x[2] - (__ldcg(T.sz + s) + M.off[src][2]);
+        const double dx = x[0] - (v.x + M.off[srci][0]), dy = x[1] - (v.y + M.off[srci][1]),
+                     dz = x[2] - (v.z + M.off[srci][2]);
         const double r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 > eps && r2 < b * b) acc[2 + p] += __ldcg(T.sq + s) * poly(sqrt(r2), b);
+        if (r2 > eps && r2 < b * b) acc[2 + p] += v.w * poly(sqrt(r2), b);
       }
       // arrivals parked in the overflow pool that belong to a source's subtree
-      const int pn = __ldcg(T.pool_n);
-      for (int e = gt; e < 2 * 36 * pn; e += gstride) {
-        const int p = e / (36 * pn), sj = (e / pn) % 36, q = e % pn;
+      const int pn = s_pn;
+      for (int e2 = gt; e2 < 2 * 36 * pn; e2 += gstride) {
+        const int p = e2 / (36 * pn), sj = (e2 / pn) % 36, q = e2 % pn;
         const ResMeta& M = meta[p];
         if (M.cnt[sj] < 0 || __ldcg(T.p_orig + q) < 0) continue;
         const int pl = __ldcg(T.p_leaf + q);
@@ -1049,14 +1109,26 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
       // (its own slot and the slot of the particle swapped into its place) or
       // moved that very particle
       const bool stale = s_acc && (h.path_o[h.depth_o - 1] != h.path_t[h.depth_t - 1] || i_next == h.i_orig);
-      s_hint = stale ? -1 : s_next;
-      if (!stale && threadIdx.x == 0 && s_next < T.n_slots) {
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(T.sx + s_next));
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(T.sy + s_next));
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(T.sz + s_next));
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(T.sq + s_next));
+      // a kept slot is loaded now; an accepted move writes other slots only,
+      // and the commit of a same-leaf move of this very particle marks it stale
+      pre.s = -1;
+      if (!stale) {
+        pre.s = s_next;
+        if (s_next < T.n_slots) {
+          pre.x = __ldcg(T.sx + s_next);
+          pre.y = __ldcg(T.sy + s_next);
+          pre.z = __ldcg(T.sz + s_next);
+          pre.q = __ldcg(T.sq + s_next);
+        } else {
+          const int pp = s_next - T.n_slots;
+          pre.x = __ldcg(T.px + pp);
+          pre.y = __ldcg(T.py + pp);
+          pre.z = __ldcg(T.pz + pp);
+          pre.q = __ldcg(T.pq + pp);
+        }
       }
       i_cur = i_next;
+      for (int c = 0; c < 3; ++c) d_cur[c] = d_next[c];
     }
     if (!s_acc) continue;
     // accept-and-update (src/tree.cpp:447-597)
@@ -1075,7 +1147,7 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
         }
       }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (blockIdx.x == G / 2 && threadIdx.x == 0) {
       P.i_orig = h.i_orig;
       P.slot = h.slot;
       P.q = h.q;
@@ -1098,7 +1170,7 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
     }
     {
       // root window: out_root += t - o
-      for (int k = gt; k < T.Hw; k += gstride) {
+      for (int k = gtr; k < T.Hw; k += gstride) {
         const double2 t = phase_at(to.root, k, T.dw), o = phase_at(oo.root, k, T.dw);
         double2 g = __ldcg(T.out_root + k);
         g = cadd(g, t);
