@@ -348,27 +348,33 @@ __device__ inline void node_center(const DevTree& T, int node, double* c) {
 }
 
 constexpr int RES_T = 128;
-constexpr int RES_CHUNK = 128;
+constexpr int RES_TCH = 64;   // targets of one work item
+constexpr int RES_SCH = 256;  // sources staged in shared memory per round
 
 // leaf near field: 1/2 sum_{i in B} q_i sum_{j in N(B), j != i} q_j res(r_ij; bs_B)
-// (eval_energy_res, src/energy.cpp:82-173). The up to 35 source boxes (self,
-// colleagues, coarse-grain) are flattened into one index range: their
-// metadata is fetched in parallel, then sources are staged in chunks.
+// (eval_energy_res, src/energy.cpp:82-173). One block per (leaf, chunk of
+// RES_TCH targets), so a large leaf is spread over several blocks; leaves are
+// listed coarse level first, so the big items start first. The up to 35
+// source boxes (self, colleagues, coarse-grain) are flattened into one index
+// range, staged in rounds of RES_SCH with their periodic offsets applied.
+// Each thread keeps one target in registers and walks a share of the staged
+// sources (a warp reads the same source: a shared-memory broadcast).
 template <int NP>
-__global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __restrict__ leaves, double* part) {
-  __shared__ double tx[RES_CHUNK], ty[RES_CHUNK], tz[RES_CHUNK], tq[RES_CHUNK];
-  __shared__ double ux[RES_CHUNK], uy[RES_CHUNK], uz[RES_CHUNK], uq[RES_CHUNK];
-  __shared__ int uslot[RES_CHUNK];
+__global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __restrict__ leaves, int ny,
+                                                    double* part) {
+  __shared__ double ux[RES_SCH], uy[RES_SCH], uz[RES_SCH], uq[RES_SCH];
+  __shared__ int uslot[RES_SCH];
   __shared__ int m_beg[36], m_pre[37];
   __shared__ double m_off[36][3];
   __shared__ double sm[32];
   const ResidualPoly<NP> poly(T);
-  const int node = leaves[blockIdx.x];
+  const int node = leaves[blockIdx.x / ny], chunk = blockIdx.x % ny;
   const int l = T.node_level[node];
   const int cnt = T.leaf_count[node];
   double e = 0;
-  if (l >= 2 && cnt > 0) {
+  if (l >= 2 && cnt > chunk * RES_TCH) {
     const double b = level_box(T, l);
+    const double b2 = b * b * (1.0 + 1e-14);  // sqrt only near or inside the cut-off
     const int tb = T.node_begin[node];
     if (threadIdx.x < 36) {
       const int src = threadIdx.x;
@@ -403,38 +409,52 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
     }
     __syncthreads();
     const int total = m_pre[36];
-    for (int t0 = 0; t0 < cnt; t0 += RES_CHUNK) {
-      const int nt = min(RES_CHUNK, cnt - t0);
-      for (int u0 = 0; u0 < total; u0 += RES_CHUNK) {
-        const int ns = min(RES_CHUNK, total - u0);
+    for (int t0 = chunk * RES_TCH; t0 < cnt; t0 += ny * RES_TCH) {
+      const int nt = min(RES_TCH, cnt - t0);
+      const int npad = nt <= 32 ? 32 : 64;
+      const int nparts = RES_T / npad;
+      const int it = threadIdx.x % npad, sp = threadIdx.x / npad;
+      const bool act = it < nt;
+      int tslot = -2;
+      double tx = 0, ty = 0, tz = 0, tq = 0;
+      if (act) {
+        tslot = tb + t0 + it;
+        tx = T.sx[tslot];
+        ty = T.sy[tslot];
+        tz = T.sz[tslot];
+        tq = T.sq[tslot];
+      }
+      double et = 0;
+      for (int u0 = 0; u0 < total; u0 += RES_SCH) {
+        const int ns = min(RES_SCH, total - u0);
         __syncthreads();
-        if (u0 == 0)
-          for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-            tx[t] = T.sx[tb + t0 + t];
-            ty[t] = T.sy[tb + t0 + t];
-            tz[t] = T.sz[tb + t0 + t];
-            tq[t] = T.sq[tb + t0 + t];
-          }
         for (int t = threadIdx.x; t < ns; t += blockDim.x) {
           const int ei = u0 + t;
-          int src = 0;
-          while (ei >= m_pre[src + 1]) ++src;
-          const int s = m_beg[src] + (ei - m_pre[src]);
-          ux[t] = T.sx[s] + m_off[src][0];
-          uy[t] = T.sy[s] + m_off[src][1];
-          uz[t] = T.sz[s] + m_off[src][2];
+          int lo = 0, hi = 36;  // largest src with m_pre[src] <= ei
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (m_pre[mid] <= ei) lo = mid;
+            else hi = mid;
+          }
+          const int s = m_beg[lo] + (ei - m_pre[lo]);
+          ux[t] = T.sx[s] + m_off[lo][0];
+          uy[t] = T.sy[s] + m_off[lo][1];
+          uz[t] = T.sz[s] + m_off[lo][2];
           uq[t] = T.sq[s];
-          uslot[t] = src == 0 ? s : -1;
+          uslot[t] = lo == 0 ? s : -1;
         }
         __syncthreads();
-        for (int pq = threadIdx.x; pq < nt * ns; pq += blockDim.x) {
-          const int it = pq / ns, js = pq % ns;
-          if (uslot[js] == tb + t0 + it) continue;  // a particle with itself
-          const double dx = tx[it] - ux[js], dy = ty[it] - uy[js], dz = tz[it] - uz[js];
-          const double r = sqrt(dx * dx + dy * dy + dz * dz);
-          if (r <= b) e += tq[it] * uq[js] * poly(r, b);
-        }
+        if (act)
+          for (int js = sp; js < ns; js += nparts) {
+            const double dx = tx - ux[js], dy = ty - uy[js], dz = tz - uz[js];
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 <= b2 && uslot[js] != tslot) {
+              const double r = sqrt(r2);
+              if (r <= b) et += uq[js] * poly(r, b);
+            }
+          }
       }
+      e += tq * et;
     }
   }
   double s = block_sum(0.5 * e, sm);
@@ -465,13 +485,19 @@ __global__ void k_sum_q2(const double* sq, int n, double* out) {
 constexpr int KSPLIT = 4096;       // particles per split-K chunk of a box
 constexpr int KSPLIT_ROOT = 2048;  // particles per chunk of the root pass
 
+// target chunks per leaf in the near-field launch: enough for a full leaf
+// with its slack (larger leaves loop over their chunks)
+int DmkTree::res_chunks() const {
+  return std::min(8, std::max(1, (n_per_leaf_ + opt_.leaf_slack + RES_TCH - 1) / RES_TCH));
+}
+
 size_t DmkTree::partials_needed() const {
   const DevTree& D = dev_;
   size_t need = 8192;
   long n_pw = D.pw_hi >= D.pw_lo ? long(D.level_start[D.pw_hi + 1]) - D.level_start[D.pw_lo] : 0;
   long ktiles = (D.H + TPB - 1) / TPB;
   need = std::max<size_t>(need, size_t(n_pw) * ktiles + 2 * size_t(n_pw) + 64);
-  need = std::max<size_t>(need, size_t(D.n_nodes) + 64);
+  need = std::max<size_t>(need, size_t(D.n_nodes) * res_chunks() + 64);
   return need;
 }
 
@@ -735,9 +761,10 @@ double DmkTree::eval_res_energy() {
   if (n_leaves_ > 0) {
     auto kern = D.n_poly == 7 ? k_residual<7> : D.n_poly == 13 ? k_residual<13> : D.n_poly == 19 ? k_residual<19>
                                                                                                  : k_residual<25>;
-    kern<<<unsigned(n_leaves_), RES_T, 0, st_>>>(D, d_leaves_, D.partials);
+    const int ny = res_chunks();
+    kern<<<unsigned(n_leaves_ * ny), RES_T, 0, st_>>>(D, d_leaves_, ny, D.partials);
     PDMK_LAUNCH_CHECK();
-    k_sum<<<1, 1024, 0, st_>>>(D.partials, n_leaves_, d_scalars_ + 2);
+    k_sum<<<1, 1024, 0, st_>>>(D.partials, n_leaves_ * ny, d_scalars_ + 2);
     PDMK_LAUNCH_CHECK();
   }
   double e = 0;

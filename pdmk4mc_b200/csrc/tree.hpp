@@ -217,6 +217,7 @@ class DmkTree {
   void layout_slots(const double* dsx, const double* dsy, const double* dsz, const double* dsq, const int* dorig,
                     const long* src_lo, int leaf_slack);
   size_t partials_needed() const;
+  int res_chunks() const;
   void launch_shift(const int* d_idx, const double* d_disp, const double* d_u, double beta, int move, int mode,
                     double* d_dE, int* d_acc);
   void launch_update();  // accept-and-update and membership commit, one launch
