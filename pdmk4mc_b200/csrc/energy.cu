@@ -146,20 +146,17 @@ __global__ void __launch_bounds__(NudftShape<NK>::THREADS)
     const double2* ez = ey + S::KC * S::DP;
     const int nk = min(S::KC, w.s_end - base);
     if (active) {
-#pragma unroll 2
+#pragma unroll 1
       for (int j = 0; j < nk; ++j) {
         const double2 a = cmul(ez[j * (NK + 1) + kz], ey[j * S::DP + ky]);
         const double2* xr = ex + j * S::DP + c0;
-        // two sweeps keep the two FMAs of each complex product independent
+        // one shared-memory load per column feeds its four FMAs; the 2 TC
+        // accumulator chains give enough independent work to hide latency
 #pragma unroll
         for (int c = 0; c < S::TC; ++c) {
           const double2 b = xr[c];
           acc[c].x = fma(a.x, b.x, acc[c].x);
           acc[c].y = fma(a.x, b.y, acc[c].y);
-        }
-#pragma unroll
-        for (int c = 0; c < S::TC; ++c) {
-          const double2 b = xr[c];
           acc[c].x = fma(-a.y, b.y, acc[c].x);
           acc[c].y = fma(a.y, b.x, acc[c].y);
         }
