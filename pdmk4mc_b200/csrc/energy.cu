@@ -441,13 +441,26 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
           uslot[t] = lo == 0 ? s : -1;
         }
         __syncthreads();
+        // two sources per step: their Horner chains are independent, so each
+        // hides the other's FMA latency
         if (act)
-          for (int js = sp; js < ns; js += nparts) {
-            const double dx = tx - ux[js], dy = ty - uy[js], dz = tz - uz[js];
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 <= b2 && uslot[js] != tslot) {
-              const double r = sqrt(r2);
-              if (r <= b) et += uq[js] * poly(r, b);
+          for (int js = sp; js < ns; js += 2 * nparts) {
+            const int j2 = js + nparts;
+            const double dxa = tx - ux[js], dya = ty - uy[js], dza = tz - uz[js];
+            const double r2a = dxa * dxa + dya * dya + dza * dza;
+            const bool ina = r2a <= b2 && uslot[js] != tslot;
+            bool inb = false;
+            double r2b = 0;
+            if (j2 < ns) {
+              const double dxb = tx - ux[j2], dyb = ty - uy[j2], dzb = tz - uz[j2];
+              r2b = dxb * dxb + dyb * dyb + dzb * dzb;
+              inb = r2b <= b2 && uslot[j2] != tslot;
+            }
+            if (ina || inb) {
+              const double ra = sqrt(ina ? r2a : 0.25 * b * b), rb = sqrt(inb ? r2b : 0.25 * b * b);
+              const double pa = poly(ra, b), pb = poly(rb, b);
+              if (ina && ra <= b) et += uq[js] * pa;
+              if (inb && rb <= b) et += uq[j2] * pb;
             }
           }
       }

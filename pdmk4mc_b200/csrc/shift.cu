@@ -1242,6 +1242,85 @@ McKernel mc_kernel(int np) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Many candidate moves against one state in one launch: one block per
+// candidate evaluates its whole dE (resolve, phase tables, window and
+// difference sums over all modes, both near-field sums, self term) and
+// reduces it inside the block, so no grid-wide partials are needed and the
+// candidates run side by side on all SMs. Candidates whose paths share boxes
+// read the shared incoming rows through L2.
+constexpr int SB_T = 256;
+
+template <int NP>
+__global__ void __launch_bounds__(SB_T) k_shift_batch(DevTree T, const int* __restrict__ idx,
+                                                      const double* __restrict__ disp, double c_window,
+                                                      double* __restrict__ dE_out) {
+  extern __shared__ double2 sm2[];
+  __shared__ Header h;
+  __shared__ double red[4][32];
+  __shared__ double c_level[MAXLV + 2];
+  const ResidualPoly<NP> poly(T);
+  if (threadIdx.x >= 2 && threadIdx.x < MAXLV + 2) {
+    const double dk = level_dk(T, threadIdx.x);
+    c_level[threadIdx.x] = dk * dk * dk / (8.0 * 3.14159265358979323846 * 3.14159265358979323846 *
+                                           3.14159265358979323846) * level_dscale(threadIdx.x);
+  }
+  const int c = blockIdx.x;
+  resolve(T, idx[c], disp + 3 * c, h);
+  const int lo_max = h.depth_o - 2, lt_max = h.depth_t - 2;
+  const int per = 3 * (2 * T.n_window + 1) + max(max(lo_max, lt_max) - 1, 0) * 3 * (2 * T.n_diff + 1);
+  Tables to, oo;
+  alloc_tables(sm2, T, oo);
+  alloc_tables(sm2 + per, T, to);
+  build_tables(T, h.xo, h.q, h.Xo, lo_max, oo, threadIdx.x, blockDim.x);
+  build_tables(T, h.xt, h.q, h.Xt, lt_max, to, threadIdx.x, blockDim.x);
+  __syncthreads();
+  double acc[4] = {0, 0, 0, 0};
+  for (int k = threadIdx.x; k < T.Hw; k += blockDim.x) {
+    const double2 t = phase_at(to.root, k, T.dw), o = phase_at(oo.root, k, T.dw);
+    const double2 g = T.out_root[k];
+    const double ar = t.x - o.x, ai = t.y - o.y, br = g.x - o.x, bi = g.y - o.y;
+    acc[0] += (ar * br + ai * bi) * T.W[k];
+  }
+  const int base = T.pw_base, d = T.dd;
+  for (int k = threadIdx.x; k < T.H; k += blockDim.x) {
+    const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
+    double sd = 0;
+    for (int l = 2; l <= lo_max; ++l) {
+      const double2 o = cmul(oo.lev[l][2][iz], cmul(oo.lev[l][1][iy], oo.lev[l][0][ix]));
+      const double2 cc = T.inc[size_t(h.path_o[l] - base) * T.H + k];
+      sd -= (o.x * cc.x - o.y * cc.y - (o.x * o.x + o.y * o.y)) * c_level[l];
+    }
+    for (int l = 2; l <= lt_max; ++l) {
+      const double2 t = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
+      const double2 cc = T.inc[size_t(h.path_t[l] - base) * T.H + k];
+      sd += (t.x * cc.x - t.y * cc.y) * c_level[l];
+    }
+    acc[1] += sd * T.D2[k];
+  }
+  const int lt = h.depth_t - 1, lo = h.depth_o - 1;
+  acc[2] = residual_sum(T, poly, h.path_t[lt], lt, h.Xt[lt], h.xt);
+  __syncthreads();  // the second call reuses the source-list arrays of the first
+  acc[3] = residual_sum(T, poly, h.path_o[lo], lo, h.Xo[lo], h.xo);
+  block_sum4(acc, red);
+  if (threadIdx.x == 0) {
+    double self = 0;
+    if (h.dr != 0) self = poly(h.dr, level_box(T, 2)) * h.q * h.q;
+    dE_out[c] = acc[0] * c_window + acc[1] + (acc[2] - acc[3]) * h.q - self;
+  }
+}
+
+using ShiftBatchKernel = void (*)(DevTree, const int*, const double*, double, double*);
+ShiftBatchKernel shift_batch_kernel(int np) {
+  switch (np) {
+    case 7: return k_shift_batch<7>;
+    case 13: return k_shift_batch<13>;
+    case 19: return k_shift_batch<19>;
+    case 25: return k_shift_batch<25>;
+    default: throw std::invalid_argument("unsupported residual polynomial");
+  }
+}
+
 // the shift kernel for a residual polynomial of np coefficients (3, 6, 9, 12 digits)
 using ShiftKernel = void (*)(DevTree, ShiftArgs);
 ShiftKernel shift_kernel(int np) {
@@ -1555,8 +1634,22 @@ void DmkTree::mc_run_device(int n_moves, const int* d_idx, const double* d_disp,
   diff_cached_ = false;
 }
 
+// All candidates in one launch of k_shift_batch (one block per candidate).
 void DmkTree::shift_batch_device(int m, const int* d_idx, const double* d_disp, double* d_dE) {
-  for (int c = 0; c < m; ++c) launch_shift(d_idx, d_disp, nullptr, 0.0, c, 0, d_dE, nullptr);
+  DevTree& D = dev_;
+  if (m <= 0) return;
+  const size_t smem = tables_smem(D, D.max_depth, 2);
+  const ShiftBatchKernel kern = shift_batch_kernel(D.n_poly);
+  static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
+  const int slot = (D.n_poly - 7) / 6;
+  if (smem > smem_set[slot]) {
+    PDMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    smem_set[slot] = smem;
+  }
+  const double pi = 3.14159265358979323846;
+  const double c_window = std::pow(D.delta_k[0], 3) / std::pow(2 * pi, 3);
+  kern<<<unsigned(m), SB_T, smem, st_>>>(D, d_idx, d_disp, c_window, d_dE);
+  PDMK_LAUNCH_CHECK();
   last_valid_ = false;
 }
 
