@@ -227,51 +227,116 @@ __global__ void k_reduce_chunks(const double2* part, const int* chunk_first, con
 }
 
 // ---------------------------------------------------------------------------
-__device__ inline int wrap_flag(int X, int d, int l) {
-  int v = X + d;
-  return v < 0 ? -1 : (v >= (1 << l) ? 1 : 0);
-}
+// inc_B = conj(out_B) + sum_C conj(out_C * exp(-i k.p L)) (form_incoming_pw,
+// src/planewave.cpp:99-155) for the 8 children of one parent at once: the
+// children's 27-box neighbourhoods lie in the 4x4x4 cube of boxes around the
+// parent, so a block stages the cube's outgoing rows for one tile of INC_KT
+// modes in shared memory (image phase applied, conjugated) and every child
+// sums its 27 cells from there. Each row tile crosses L2 once per cube
+// instead of once per receiving box. The energy partial of a block sums its
+// non-leaf children, which share one level.
+constexpr int INC_KT = 32;
 
-// inc_B = conj(out_B) + sum_C conj(out_C * exp(-i k.p L)), with the energy
-// sum Re(out_B inc_B) D_2 per (box, k tile); ktile-major grid order keeps the
-// colleagues' tiles resident in L2.
-__global__ void k_incoming(DevTree T, const int* __restrict__ boxes, int nboxes, int write_inc, double* part) {
+// Grid: ngroups x slots blocks; block (slot, g) handles the tiles slot,
+// slot + slots, ... of group g, so its set-up (the cube's box list) is paid
+// once, and the groups sharing a slot walk the same tiles together (their
+// shared rows meet in L2).
+__global__ void __launch_bounds__(8 * INC_KT) k_incoming_sib(DevTree T, const int* __restrict__ parents, int ngroups,
+                                                              int slots, double* part) {
+  __shared__ double2 w[64][INC_KT];
+  __shared__ int s_src[64];
+  __shared__ signed char s_f[64][3];
   __shared__ double sm[32];
-  const int tile = blockIdx.x / nboxes, b = blockIdx.x % nboxes;
-  const int node = boxes[b];
-  const int l = T.node_level[node];
-  const uint64_t p = T.node_prefix[node];
-  const int X = compact3(p), Y = compact3(p >> 1), Z = compact3(p >> 2);
-  const int n = T.n_diff, d = T.dd;
-  const int k = tile * blockDim.x + threadIdx.x;
+  const int slot = blockIdx.x / ngroups, g = blockIdx.x % ngroups;
+  const int parent = parents[g];
+  const int c0 = T.node_child0[parent];
+  const int l = T.node_level[parent] + 1;
   const int base = T.pw_base;
-  double e = 0;
-  if (k < T.H) {
-    const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
-    const int two_l_mod3 = (l & 1) ? 2 : 1;
-    const double2* outB = T.out + size_t(node - base) * T.H;
-    double2 acc = T.node_count[node] > 0 ? cconj(outB[k]) : make_double2(0, 0);
-    const int* col = T.col27 + size_t(node) * 27;
-    for (int dir = 0; dir < 27; ++dir) {
-      int j = col[dir];
-      if (j < 0 || T.node_count[j] == 0) continue;
-      int dx = dir % 3 - 1, dy = (dir / 3) % 3 - 1, dz = dir / 9 - 1;
-      // image offset of the source colleague as seen from B (periodic_shift(c_C, c_B))
-      int px = wrap_flag(X, dx, l), py = wrap_flag(Y, dy, l), pz = wrap_flag(Z, dz, l);
-      double2 v = T.out[size_t(j - base) * T.H + k];
-      if (px | py | pz) {
-        int sgn = ((ix - n) * px + (iy - n) * py + (iz - n) * pz) * two_l_mod3;
-        // exp(-i 2 pi sgn / 3) = w6^{-2 sgn}
-        v = cmul(v, root6(-2 * (sgn % 3)));
-      }
-      acc = cadd(acc, cconj(v));
+  const uint64_t pp = T.node_prefix[parent];
+  const int P[3] = {int(compact3(pp)), int(compact3(pp >> 1)), int(compact3(pp >> 2))};
+  if (threadIdx.x < 64) {
+    const int t = int(threadIdx.x);
+    s_src[t] = -1;
+    const int o[3] = {t & 3, (t >> 2) & 3, t >> 4};
+    for (int a = 0; a < 3; ++a) {
+      const int v = 2 * P[a] - 1 + o[a];
+      s_f[t][a] = static_cast<signed char>(v < 0 ? -1 : (v >= (1 << l) ? 1 : 0));
     }
-    if (write_inc) T.inc[size_t(node - base) * T.H + k] = acc;
-    const double2 o = outB[k];
-    e = (o.x * acc.x - o.y * acc.y) * T.D2[k];
+  }
+  __syncthreads();
+  // cube cells from the children's colleague lists (a cell seen from two
+  // children names the same box)
+  if (threadIdx.x < 216) {
+    const int c = threadIdx.x / 27, dir = threadIdx.x % 27;
+    const int child = c0 + c;
+    const int j = dir == 13 ? child : T.col27[size_t(child) * 27 + dir];
+    const int cell = ((c & 1) + 1 + dir % 3 - 1) + 4 * (((c >> 1) & 1) + 1 + (dir / 3) % 3 - 1) +
+                     16 * (((c >> 2) & 1) + 1 + dir / 9 - 1);
+    if (j >= 0 && T.node_count[j] > 0) s_src[cell] = j - base;
+  }
+  const int n = T.n_diff, d = T.dd;
+  const int two_l = (l & 1) ? 2 : 1;
+  const int kk = threadIdx.x % INC_KT, part8 = threadIdx.x / INC_KT;  // staging: one mode, cells part8 + 8 i
+  const int c = part8;                                                // summing: child c
+  const int child = c0 + c;
+  const bool recv = T.node_child0[child] >= 0;
+  const int cx = (c & 1) + 1, cy = ((c >> 1) & 1) + 1, cz = ((c >> 2) & 1) + 1;
+  __syncthreads();
+  double e = 0;
+  const int ktiles = (T.H + INC_KT - 1) / INC_KT;
+  for (int tile = slot; tile < ktiles; tile += slots) {
+    const int k = tile * INC_KT + kk;
+    const bool kin = k < T.H;
+    const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
+    const int a0 = ((ix - n) % 3 + 3) % 3, a1 = ((iy - n) % 3 + 3) % 3, a2 = ((iz - n) % 3 + 3) % 3;
+    double2 v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int row = s_src[part8 + 8 * i];
+      v[i] = (row >= 0 && kin) ? T.out[size_t(row) * T.H + k] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int cell = part8 + 8 * i;
+      const signed char* f = s_f[cell];
+      // exp(-i 2 pi sgn / 3) = w6^{-2 sgn}, sgn = (k - n).f 2^l; the sum lies in [-12, 12]
+      const int e3 = ((a0 * f[0] + a1 * f[1] + a2 * f[2]) * two_l + 12) % 3;
+      w[cell][kk] = cconj(e3 == 0 ? v[i] : cmul(v[i], root6(-2 * e3)));
+    }
+    __syncthreads();
+    if (kin && recv) {
+      double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int dir = 0; dir < 27; ++dir) {
+        const int cell = (cx + dir % 3 - 1) + 4 * (cy + (dir / 3) % 3 - 1) + 16 * (cz + dir / 9 - 1);
+        acc = cadd(acc, w[cell][kk]);
+      }
+      T.inc[size_t(child - base) * T.H + k] = acc;
+      const double2 o = T.out[size_t(child - base) * T.H + k];
+      e += (o.x * acc.x - o.y * acc.y) * T.D2[k];
+    }
+    __syncthreads();
   }
   double s = block_sum(e, sm);
   if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// E_diff from the sibling-tiled partials: sum over groups C_l dscale_l
+// sum_tiles part, minus sum over non-leaf boxes Q_B S_l
+__global__ void k_diff_finish_sib(DevTree T, const int* __restrict__ parents, int ngroups, int ktiles,
+                                  const double* part, const int* __restrict__ boxes, int nboxes, const double* q2,
+                                  const double* Cl, const double* Sl, double* out) {
+  __shared__ double sm[32];
+  double e = 0;
+  for (int g = threadIdx.x; g < ngroups; g += blockDim.x) {
+    const int l = T.node_level[parents[g]] + 1;
+    double t = 0;
+    for (int tile = 0; tile < ktiles; ++tile) t += part[size_t(tile) * ngroups + g];
+    e += Cl[l] * level_dscale(l) * t;
+  }
+  for (int b = threadIdx.x; b < nboxes; b += blockDim.x) e -= q2[b] * Sl[T.node_level[boxes[b]]];
+  double s = block_sum(e, sm);
+  if (threadIdx.x == 0) *out = s;
 }
 
 // Re sum out_B inc_B D_2 per (box, k tile) on the stored incoming expansions
@@ -507,6 +572,8 @@ size_t DmkTree::partials_needed() const {
   long n_pw = D.pw_hi >= D.pw_lo ? long(D.level_start[D.pw_hi + 1]) - D.level_start[D.pw_lo] : 0;
   long ktiles = (D.H + TPB - 1) / TPB;
   need = std::max<size_t>(need, size_t(n_pw) * ktiles + 2 * size_t(n_pw) + 64);
+  // sibling-tiled incoming: at most one group per 8 expansion boxes
+  need = std::max<size_t>(need, size_t((D.H + INC_KT - 1) / INC_KT) * size_t(n_pw / 8 + 1) + 2 * size_t(n_pw) + 64);
   need = std::max<size_t>(need, size_t(D.n_nodes) * res_chunks() + 64);
   return need;
 }
@@ -688,6 +755,18 @@ void DmkTree::prepare_box_lists() {
   std::vector<int> leaves;
   for (int id = D.level_start[2]; id < D.n_nodes; ++id)
     if (c0[id] < 0) leaves.push_back(id);
+  // parents whose children carry expansions and include a non-leaf box
+  std::vector<int> groups;
+  if (D.pw_hi >= D.pw_lo)
+    for (int id = D.level_start[D.pw_lo - 1]; id < D.level_start[D.pw_hi]; ++id) {
+      if (c0[id] < 0) continue;
+      bool any = false;
+      for (int c = 0; c < 8; ++c) any = any || c0[c0[id] + c] >= 0;
+      if (any) groups.push_back(id);
+    }
+  n_groups_ = int(groups.size());
+  d_groups_ = static_cast<int*>(alloc(sizeof(int) * (n_groups_ + 1)));
+  PDMK_CUDA(cudaMemcpyAsync(d_groups_, groups.data(), sizeof(int) * n_groups_, cudaMemcpyHostToDevice, st_));
   n_nonleaf_ = int(nonleaf.size());
   n_leaves_ = int(leaves.size());
   d_nonleaf_ = static_cast<int*>(alloc(sizeof(int) * (n_nonleaf_ + 1)));
@@ -722,18 +801,26 @@ void DmkTree::run_incoming(bool write_inc) {
     return;
   }
   const int ktiles = (D.H + TPB - 1) / TPB;
+  const size_t n_part = std::max(size_t(ktiles) * n_nonleaf_, size_t((D.H + INC_KT - 1) / INC_KT) * n_groups_);
   double* part = D.partials;
-  double* q2 = D.partials + size_t(ktiles) * n_nonleaf_;
-  if (write_inc) {
-    k_incoming<<<unsigned(ktiles * n_nonleaf_), TPB, 0, st_>>>(D, d_nonleaf_, n_nonleaf_, 1, part);
-  } else {
-    k_tridot<<<unsigned(ktiles * n_nonleaf_), TPB, 0, st_>>>(D, d_nonleaf_, n_nonleaf_, part);
-  }
-  PDMK_LAUNCH_CHECK();
+  double* q2 = D.partials + n_part;
   k_box_q2<<<unsigned(n_nonleaf_), TPB, 0, st_>>>(D, d_nonleaf_, q2);
   PDMK_LAUNCH_CHECK();
-  k_diff_finish<<<1, 1024, 0, st_>>>(D, d_nonleaf_, n_nonleaf_, ktiles, part, q2, d_Cl_, d_Sl_, d_scalars_ + 1);
-  PDMK_LAUNCH_CHECK();
+  if (write_inc) {
+    // about four resident waves of blocks, each walking a strided set of tiles
+    const int kt = (D.H + INC_KT - 1) / INC_KT;
+    const int slots = std::max(1, std::min(kt, (4 * 8 * 148 + n_groups_ - 1) / n_groups_));
+    k_incoming_sib<<<unsigned(slots * n_groups_), 8 * INC_KT, 0, st_>>>(D, d_groups_, n_groups_, slots, part);
+    PDMK_LAUNCH_CHECK();
+    k_diff_finish_sib<<<1, 1024, 0, st_>>>(D, d_groups_, n_groups_, slots, part, d_nonleaf_, n_nonleaf_, q2, d_Cl_,
+                                           d_Sl_, d_scalars_ + 1);
+    PDMK_LAUNCH_CHECK();
+  } else {
+    k_tridot<<<unsigned(ktiles * n_nonleaf_), TPB, 0, st_>>>(D, d_nonleaf_, n_nonleaf_, part);
+    PDMK_LAUNCH_CHECK();
+    k_diff_finish<<<1, 1024, 0, st_>>>(D, d_nonleaf_, n_nonleaf_, ktiles, part, q2, d_Cl_, d_Sl_, d_scalars_ + 1);
+    PDMK_LAUNCH_CHECK();
+  }
 }
 
 void DmkTree::form_incoming_pw() {

@@ -257,6 +257,8 @@ class DmkTree {
   int n_nonleaf_ = 0, n_leaves_ = 0;
   int* d_nonleaf_ = nullptr;  // non-leaf nodes of the expansion levels
   int* d_leaves_ = nullptr;   // leaves at levels >= 2
+  int n_groups_ = 0;
+  int* d_groups_ = nullptr;   // parents of expansion boxes with a non-leaf child
   double* d_Cl_ = nullptr;
   double* d_Sl_ = nullptr;
   double* d_scalars_ = nullptr;
