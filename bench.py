@@ -183,7 +183,7 @@ def run_reference(args, rank, ws):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "moves/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * W["moves_per_step"] / v,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(W, parallelism="replicas"),
+        "config": dict(W, parallelism="replicas" if ws > 1 else "single"),
         "full_energy_evals_per_s": float(np.mean(ee)),
         "cpu_baseline": {"value": v, "unit": "moves/s", "cores": 1, "kind": "port",
                          "sample": f"{res['moves']} sequential Metropolis moves (1 thread, as the reference's "
@@ -288,6 +288,9 @@ def run_b200(args, rank, ws):
                   f"{M} moves per launch)")
         bytes_per_launch = (work[1] + work[2]) / max(upd_n, 1)
     achieved = bytes_per_launch / (upd_ms / upd_n / 1e3) / 1e9 if upd_n else None
+    # DRAM traffic of k_mc from one ncu capture of a 256-move launch on this
+    # workload (966 MB read + 1 322 MB written), scaled to a launch by moves
+    traffic = None if args.mc_mode == "graph" else (966.42e6 + 1321.68e6) / 256 * M
 
     # end to end through the C-ABI with host buffers (copies inside the timed region)
     e2e_t = []
@@ -322,7 +325,9 @@ def run_b200(args, rank, ws):
             "full_energy_evals_per_s": energy_per_s,
             "accept_rate": work[0] / (M * args.steps),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                         "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 256-move k_mc "
+                                           "launch, scaled by moves per launch" if traffic else None,
                          "kernel": kernel,
                          "timed_launches": int(upd_n),
                          "peak_source": peak_kind},
