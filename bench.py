@@ -250,7 +250,7 @@ def run_b200(args, rank, ws):
                                device_inputs=(d_r.data_ptr(), d_q.data_ptr(), n))
             ef.form_outgoing_pw()
             ef.form_incoming_pw()
-            ef.eval_energy()
+            e_dmk = ef.eval_energy()
             ee1.record(estream)
             torch.cuda.synchronize()
             ef.close()
@@ -308,6 +308,17 @@ def run_b200(args, rank, ws):
     te2e = all_max(float(np.sum(e2e_t)), ws)
     e2e_val = ws * M * args.steps / te2e
 
+    # accuracy of the timed energy against the stored FP64 Ewald energy of
+    # this workload (tests/golden/bench_ewald.json, made by the oracle)
+    accuracy = None
+    gp = os.path.join(ROOT, "tests", "golden", "bench_ewald.json")
+    if rank == 0 and os.path.exists(gp):
+        g = json.load(open(gp))
+        if g["workload"]["N"] == n and g["workload"]["L"] == L and g["workload"]["seed"] == 1:
+            ew = g["ewald"]["energy"]
+            accuracy = {"energy_dmk": e_dmk, "energy_ewald_fp64": ew, "rel_err": abs(e_dmk - ew) / abs(ew),
+                        "ewald": "oracle FP64 Ewald, s = 5, stored"}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         res = cpu_baseline_sample(W)
@@ -326,6 +337,7 @@ def run_b200(args, rank, ws):
                            l2="256 MB written before each step; the 0.56 GB of expansions exceed the 126 MB L2"),
             "full_energy_evals_per_s": energy_per_s,
             "accept_rate": work[0] / (M * args.steps),
+            "accuracy": accuracy,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 256-move k_mc "

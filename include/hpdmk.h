@@ -168,6 +168,13 @@ int hpdmk_set_mc_mode(hpdmk_tree tree, int mode);
 int hpdmk_mc_run_device(hpdmk_tree tree, int n, const int *d_i, const double *d_d, const double *d_u, double beta,
                         double *d_dE, int *d_accepted);
 
+/* FP64 Ewald energy of the current particles, the comparator for the DMK
+ * energy (reference: the Ewald summation of src/ewald.cpp:17-223, there on
+ * the CPU): real-space erfc sum with the cut-off at one tree level's box size,
+ * reciprocal sum over the structure factor, self term; truncation near 1e-12
+ * relative. parts (may be NULL) receives real, reciprocal and self terms. */
+int hpdmk_ewald_energy(hpdmk_tree tree, double *energy, double *parts);
+
 /* Current positions in the caller's original order, r[3n]. */
 int hpdmk_get_positions(hpdmk_tree tree, double *r);
 

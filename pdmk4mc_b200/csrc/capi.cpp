@@ -393,6 +393,14 @@ int hpdmk_get_timing(hpdmk_tree t, double* out, int reset) {
   });
 }
 
+int hpdmk_ewald_energy(hpdmk_tree t, double* energy, double* parts) {
+  if (!t || !energy) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  return guarded([&]() {
+    *energy = H(t)->tree->ewald_energy(parts);
+    return ok();
+  });
+}
+
 int hpdmk_get_launch_count(long long* out) {
   if (!out) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
   *out = pdmk::g_launch_count.load();

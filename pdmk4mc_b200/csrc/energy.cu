@@ -65,7 +65,8 @@ struct NudftShape {
   static constexpr int TMAX = 512;
   static constexpr int TILES = (WORK + TMAX - 1) / TMAX;
   static constexpr int THREADS = ((WORK + TILES - 1) / TILES + 31) / 32 * 32;
-  static constexpr int KC = 32;                       // particles per shared-memory chunk
+  // particles per shared-memory chunk: 32, or 16 when 32 would not fit
+  static constexpr int KC = 2 * 32 * (2 * DP + NK + 1) * 16 > 200 * 1024 ? 16 : 32;
   static constexpr int SMEM = 2 * KC * (2 * DP + NK + 1) * int(sizeof(double2));  // double-buffered
 };
 
@@ -213,6 +214,8 @@ void dispatch_nudft(int nk, const NudftWork* d_work, int nwork, const DevTree& T
     case 17: launch_nudft<17>(d_work, nwork, T, st); break;
     case 19: launch_nudft<19>(d_work, nwork, T, st); break;
     case 26: launch_nudft<26>(d_work, nwork, T, st); break;
+    case 32: launch_nudft<32>(d_work, nwork, T, st); break;  // Ewald structure factor, level 2
+    case 64: launch_nudft<64>(d_work, nwork, T, st); break;  // Ewald structure factor, level 3
     default: throw std::invalid_argument("unsupported mode count");
   }
 }
@@ -227,6 +230,8 @@ int nudft_tiles(int nk) {
     case 17: return NudftShape<17>::TILES;
     case 19: return NudftShape<19>::TILES;
     case 26: return NudftShape<26>::TILES;
+    case 32: return NudftShape<32>::TILES;
+    case 64: return NudftShape<64>::TILES;
     default: throw std::invalid_argument("unsupported mode count");
   }
 }
@@ -551,6 +556,130 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
   }
   double s = block_sum(0.5 * e, sm);
   if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 Ewald comparator (the reference's Ewald summation, src/ewald.cpp:17-223):
+// E = 1/2 sum_{i != j, images} q_i q_j erfc(alpha r)/r
+//   + (2 pi / V) sum_{k != 0} exp(-k^2 / (4 alpha^2)) / k^2 |S(k)|^2
+//   - alpha / sqrt(pi) sum_i q_i^2,  S(k) = sum_j q_j exp(i k.r_j).
+// The real-space cut-off is the box size of one tree level, so the 27 boxes
+// of that level around a box hold every pair; S(k) comes from the NUDFT
+// kernel (the conjugate, which leaves |S|^2 unchanged).
+
+// real space: one block per (box, chunk of RES_TCH targets), as the near field
+__global__ void __launch_bounds__(RES_T) k_ewald_real(DevTree T, int level, int ny, double alpha, double rc,
+                                                      double* part) {
+  __shared__ double ux[RES_SCH], uy[RES_SCH], uz[RES_SCH], uq[RES_SCH];
+  __shared__ int uslot[RES_SCH];
+  __shared__ int m_beg[27], m_pre[28];
+  __shared__ double m_off[27][3];
+  __shared__ double sm[32];
+  const int node = T.level_start_d[level] + int(blockIdx.x) / ny, chunk = int(blockIdx.x) % ny;
+  const int tb = T.node_begin[node];
+  const int cnt = T.node_end[node] - tb;  // slots, empty ones carry q = 0
+  double e = 0;
+  if (cnt > chunk * RES_TCH) {
+    const double b = level_box(T, level);
+    const double rc2 = rc * rc;
+    if (threadIdx.x < 27) {
+      const int dir = threadIdx.x;
+      const int j = dir == 13 ? node : T.col27[size_t(node) * 27 + dir];
+      int beg = 0, n = 0;
+      double off[3] = {0, 0, 0};
+      if (j >= 0) {
+        double ci[3], cj[3];
+        node_center(T, node, ci);
+        node_center(T, j, cj);
+        for (int dd = 0; dd < 3; ++dd) off[dd] = -periodic_shift_d(ci[dd], cj[dd], T.L, b, b) * T.L;
+        beg = T.node_begin[j];
+        n = T.node_end[j] - beg;
+      }
+      m_beg[dir] = beg;
+      m_pre[dir] = n;
+      for (int dd = 0; dd < 3; ++dd) m_off[dir][dd] = off[dd];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int src = 0; src < 27; ++src) {
+        const int n = m_pre[src];
+        m_pre[src] = acc;
+        acc += n;
+      }
+      m_pre[27] = acc;
+    }
+    __syncthreads();
+    const int total = m_pre[27];
+    for (int t0 = chunk * RES_TCH; t0 < cnt; t0 += ny * RES_TCH) {
+      const int nt = min(RES_TCH, cnt - t0);
+      const int npad = nt <= 32 ? 32 : 64;
+      const int nparts = RES_T / npad;
+      const int it = threadIdx.x % npad, sp = threadIdx.x / npad;
+      const bool act = it < nt;
+      int tslot = -2;
+      double tx = 0, ty = 0, tz = 0, tq = 0;
+      if (act) {
+        tslot = tb + t0 + it;
+        tx = T.sx[tslot];
+        ty = T.sy[tslot];
+        tz = T.sz[tslot];
+        tq = T.sq[tslot];
+      }
+      double et = 0;
+      for (int u0 = 0; u0 < total; u0 += RES_SCH) {
+        const int ns = min(RES_SCH, total - u0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < ns; t += blockDim.x) {
+          const int ei = u0 + t;
+          int lo = 0, hi = 27;
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (m_pre[mid] <= ei) lo = mid;
+            else hi = mid;
+          }
+          const int sl = m_beg[lo] + (ei - m_pre[lo]);
+          ux[t] = T.sx[sl] + m_off[lo][0];
+          uy[t] = T.sy[sl] + m_off[lo][1];
+          uz[t] = T.sz[sl] + m_off[lo][2];
+          uq[t] = T.sq[sl];
+          uslot[t] = sl;
+        }
+        __syncthreads();
+        if (act && tq != 0.0)
+          for (int js = sp; js < ns; js += nparts) {
+            const double dx = tx - ux[js], dy = ty - uy[js], dz = tz - uz[js];
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 < rc2 && uslot[js] != tslot && uq[js] != 0.0) {
+              const double r = sqrt(r2);
+              et += uq[js] * erfc(alpha * r) / r;
+            }
+          }
+      }
+      e += tq * et;
+    }
+  }
+  double sum = block_sum(0.5 * e, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = sum;
+}
+
+// reciprocal space over the stored half grid kz <= 0 (kz < 0 stands for its
+// mirror too)
+__global__ void k_ewald_recip(const double2* __restrict__ S, int nk, double dk, double alpha, double* part) {
+  __shared__ double sm[32];
+  const int d = 2 * nk + 1;
+  const long H = long(d) * d * (nk + 1);
+  double e = 0;
+  for (long k = long(blockIdx.x) * blockDim.x + threadIdx.x; k < H; k += long(gridDim.x) * blockDim.x) {
+    const int ix = int(k % d), iy = int((k / d) % d), iz = int(k / (long(d) * d));
+    const int mx = ix - nk, my = iy - nk, mz = iz - nk;
+    if ((mx | my | mz) == 0) continue;
+    const double k2 = dk * dk * double(mx * mx + my * my + mz * mz);
+    const double2 v = S[k];
+    e += (mz < 0 ? 2.0 : 1.0) * exp(-k2 / (4.0 * alpha * alpha)) / k2 * (v.x * v.x + v.y * v.y);
+  }
+  const double sum = block_sum(e, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = sum;
 }
 
 __global__ void k_sum(const double* part, int n, double* out) {
@@ -896,6 +1025,98 @@ EnergyParts DmkTree::eval_energy() {
   p.diff = eval_diff_energy();
   p.res = eval_res_energy();
   return p;
+}
+
+// FP64 Ewald energy of the current particles (comparator; s = 5: erfc(5) and
+// exp(-25) put the truncation near 1e-12 relative). The real-space cut-off is
+// the box size of level 2, or of level 3 when that level is complete and the
+// system is large; the k cube then needs 32 or 64 modes per axis half.
+double DmkTree::ewald_energy(double* parts) {
+  ensure_packed();
+  DevTree& D = dev_;
+  const double s = 5.0, pi = 3.14159265358979323846;
+  const bool l3 = D.max_depth > 4 && D.level_start[4] - D.level_start[3] == 512 && D.n_slots > 300000;
+  const int le = l3 ? 3 : 2;
+  const int nk = l3 ? 64 : 32;
+  const double rc = std::ldexp(L_, -le), alpha = s / rc, dk = 2 * pi / L_;
+  const int nbox = D.level_start[le + 1] - D.level_start[le];
+  // chunks of targets per box: enough for the fullest box of the level
+  std::vector<int> nb(nbox), ne(nbox);
+  PDMK_CUDA(cudaMemcpyAsync(nb.data(), D.node_begin + D.level_start[le], 4 * nbox, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaMemcpyAsync(ne.data(), D.node_end + D.level_start[le], 4 * nbox, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  int maxc = 1;
+  for (int b = 0; b < nbox; ++b) maxc = std::max(maxc, ne[b] - nb[b]);
+  const int ny = (maxc + RES_TCH - 1) / RES_TCH;
+  // structure factor by the NUDFT over all slots, split in chunks
+  const int Hs = (2 * nk + 1) * (2 * nk + 1) * (nk + 1);
+  const int kspl = std::max(4096, (D.n_slots + 295) / 296);
+  const int nch = std::max(1, (D.n_slots + kspl - 1) / kspl);
+  const int tiles = nudft_tiles(nk);
+  std::vector<NudftWork> wl;
+  for (int c = 0; c < nch; ++c) {
+    NudftWork w{};
+    w.cx = w.cy = w.cz = 0.5 * L_;
+    w.dk = dk;
+    w.M = 3;  // exp(-i k L/2) = (-1)^m: the root's decentring
+    w.s_begin = c * kspl;
+    w.s_end = std::min(D.n_slots, (c + 1) * kspl);
+    for (int t = 0; t < tiles; ++t) {
+      w.row_tile = t;
+      wl.push_back(w);
+    }
+  }
+  double2* part = nullptr;
+  double2* S = nullptr;
+  NudftWork* d_work = nullptr;
+  const int nblk_real = nbox * ny, nblk_rec = 1024;
+  double* sums = nullptr;
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double2) * size_t(Hs) * nch, st_));
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&S), sizeof(double2) * size_t(Hs), st_));
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_work), sizeof(NudftWork) * wl.size(), st_));
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&sums), sizeof(double) * (nblk_real + nblk_rec + 8), st_));
+  for (size_t i = 0; i < wl.size(); ++i) wl[i].out = part + size_t(i / tiles) * Hs;
+  PDMK_CUDA(cudaMemcpyAsync(d_work, wl.data(), sizeof(NudftWork) * wl.size(), cudaMemcpyHostToDevice, st_));
+  dispatch_nudft(nk, d_work, int(wl.size()), D, st_);
+  {
+    int* d_meta;
+    double2** d_outs;
+    const int meta[2] = {0, nch};
+    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_meta), sizeof(int) * 2, st_));
+    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_outs), sizeof(double2*), st_));
+    PDMK_CUDA(cudaMemcpyAsync(d_meta, meta, sizeof(meta), cudaMemcpyHostToDevice, st_));
+    PDMK_CUDA(cudaMemcpyAsync(d_outs, &S, sizeof(double2*), cudaMemcpyHostToDevice, st_));
+    k_reduce_chunks<<<dim3(grid_for(Hs), 1u), TPB, 0, st_>>>(part, d_meta, d_meta + 1, d_outs, Hs);
+    PDMK_LAUNCH_CHECK();
+    PDMK_CUDA(cudaFreeAsync(d_meta, st_));
+    PDMK_CUDA(cudaFreeAsync(d_outs, st_));
+  }
+  k_ewald_recip<<<unsigned(nblk_rec), TPB, 0, st_>>>(S, nk, dk, alpha, sums + nblk_real);
+  PDMK_LAUNCH_CHECK();
+  k_ewald_real<<<unsigned(nblk_real), RES_T, 0, st_>>>(D, le, ny, alpha, rc, sums);
+  PDMK_LAUNCH_CHECK();
+  k_sum<<<1, 1024, 0, st_>>>(sums, nblk_real, sums + nblk_real + nblk_rec);
+  PDMK_LAUNCH_CHECK();
+  k_sum<<<1, 1024, 0, st_>>>(sums + nblk_real, nblk_rec, sums + nblk_real + nblk_rec + 1);
+  PDMK_LAUNCH_CHECK();
+  k_sum_q2<<<1, 1024, 0, st_>>>(D.sq, D.n_slots, sums + nblk_real + nblk_rec + 2);
+  PDMK_LAUNCH_CHECK();
+  double r3[3];
+  PDMK_CUDA(cudaMemcpyAsync(r3, sums + nblk_real + nblk_rec, sizeof(r3), cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaFreeAsync(part, st_));
+  PDMK_CUDA(cudaFreeAsync(S, st_));
+  PDMK_CUDA(cudaFreeAsync(d_work, st_));
+  PDMK_CUDA(cudaFreeAsync(sums, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  const double e_real = r3[0];
+  const double e_rec = 2 * pi / (L_ * L_ * L_) * r3[1];
+  const double e_self = -alpha / std::sqrt(pi) * r3[2];
+  if (parts) {
+    parts[0] = e_real;
+    parts[1] = e_rec;
+    parts[2] = e_self;
+  }
+  return e_real + e_rec + e_self;
 }
 
 }  // namespace pdmk

@@ -179,6 +179,8 @@ class DmkTree {
   double eval_window_energy();
   double eval_diff_energy();
   double eval_res_energy();
+  // FP64 Ewald energy of the current particles (comparator); parts: real, reciprocal, self
+  double ewald_energy(double* parts = nullptr);
   // single move through the drop-in API: host scalars in, host scalar out
   double eval_shift_energy(long i, double dx, double dy, double dz, double* parts = nullptr);
   void update_shift(long i, double dx, double dy, double dz);

@@ -91,6 +91,8 @@ def load_library():
                                          ctypes.c_void_p, ctypes.c_void_p]
     L.hpdmk_get_stream.restype = ctypes.c_int
     L.hpdmk_get_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    L.hpdmk_ewald_energy.restype = ctypes.c_int
+    L.hpdmk_ewald_energy.argtypes = [ctypes.c_void_p, _dp, _dp]
     L.hpdmk_set_mc_mode.restype = ctypes.c_int
     L.hpdmk_set_mc_mode.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.hpdmk_set_timing.restype = ctypes.c_int
@@ -294,6 +296,13 @@ class HPDMKPtTree:
 
     def set_timing(self, on: bool):
         _check(load_library().hpdmk_set_timing(self._h, 1 if on else 0))
+
+    def ewald_energy(self):
+        """FP64 Ewald energy of the current particles and its (real, reciprocal, self) parts."""
+        e = ctypes.c_double(0.0)
+        parts = np.zeros(3)
+        _check(load_library().hpdmk_ewald_energy(self._h, ctypes.byref(e), _p(parts)))
+        return e.value, parts
 
     def set_mc_mode(self, mode):
         """MC_PERSISTENT (one cooperative launch, default) or MC_GRAPH (graphs of launch pairs)."""
