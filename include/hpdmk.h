@@ -168,6 +168,15 @@ int hpdmk_set_mc_mode(hpdmk_tree tree, int mode);
 int hpdmk_mc_run_device(hpdmk_tree tree, int n, const int *d_i, const double *d_d, const double *d_u, double beta,
                         double *d_dE, int *d_accepted);
 
+/* Tree maintenance (no counterpart in the reference, which keeps the tree
+ * built at construction and patches only its two lowest levels on moves,
+ * src/tree.cpp:583-596): rebuild the octree, its neighbour lists and the
+ * outgoing and incoming expansions from the current particle positions, so
+ * that leaves are back at n_per_leaf after many moves. The handle and the
+ * particles' original indices stay; the result equals a tree built from
+ * hpdmk_get_positions. Runs on the device. */
+int hpdmk_tree_rebuild(hpdmk_tree tree);
+
 /* FP64 Ewald energy of the current particles, the comparator for the DMK
  * energy (reference: the Ewald summation of src/ewald.cpp:17-223, there on
  * the CPU): real-space erfc sum with the cut-off at one tree level's box size,

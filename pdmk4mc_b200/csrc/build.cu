@@ -943,6 +943,38 @@ void DmkTree::export_sorted_order(long* out) const {
     if (so[s] >= 0) out[k++] = so[s];
 }
 
+namespace {
+// positions (xyz-interleaved) and charges in the caller's original order,
+// from the slots and the overflow pool
+__global__ void k_gather_orig(int n, const int* orig_slot, int n_slots, const double* sx, const double* sy,
+                              const double* sz, const double* sq, const double* px, const double* py,
+                              const double* pz, const double* pq, double* r, double* q) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = orig_slot[i];
+  if (s < n_slots) {
+    r[3 * i] = sx[s];
+    r[3 * i + 1] = sy[s];
+    r[3 * i + 2] = sz[s];
+    q[i] = sq[s];
+  } else {
+    const int p = s - n_slots;
+    r[3 * i] = px[p];
+    r[3 * i + 1] = py[p];
+    r[3 * i + 2] = pz[p];
+    q[i] = pq[p];
+  }
+}
+}  // namespace
+
+void DmkTree::gather_device(double* d_r, double* d_q) const {
+  const DevTree& D = dev_;
+  const int n = int(N_);
+  k_gather_orig<<<unsigned((n + 255) / 256), 256, 0, st_>>>(n, D.orig_slot, D.n_slots, D.sx, D.sy, D.sz, D.sq, D.px,
+                                                            D.py, D.pz, D.pq, d_r, d_q);
+  PDMK_LAUNCH_CHECK();
+}
+
 void DmkTree::export_positions(double* r) const {
   const int ns = dev_.n_slots;
   std::vector<double> x(ns), y(ns), z(ns);

@@ -393,6 +393,32 @@ int hpdmk_get_timing(hpdmk_tree t, double* out, int reset) {
   });
 }
 
+int hpdmk_tree_rebuild(hpdmk_tree t) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  Handle* h = H(t);
+  return guarded([&]() {
+    const pdmk::DmkTree& old = *h->tree;
+    const long n = old.n_particles();
+    double* d_r = nullptr;
+    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_r), sizeof(double) * 4 * size_t(n), h->stream));
+    double* d_q = d_r + 3 * n;
+    old.gather_device(d_r, d_q);
+    try {
+      auto nt = std::make_unique<pdmk::DmkTree>(old.box(), old.n_per_leaf(), old.digits(), n, d_r, d_q, true,
+                                                old.options(), h->stream);
+      nt->set_mc_mode(old.mc_mode());  // the caller's settings carry over
+      h->tree = std::move(nt);
+    } catch (...) {
+      cudaFreeAsync(d_r, h->stream);
+      throw;
+    }
+    PDMK_CUDA(cudaFreeAsync(d_r, h->stream));
+    h->tree->form_outgoing_pw();
+    h->tree->form_incoming_pw();
+    return ok();
+  });
+}
+
 int hpdmk_ewald_energy(hpdmk_tree t, double* energy, double* parts) {
   if (!t || !energy) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
   return guarded([&]() {

@@ -205,6 +205,13 @@ class DmkTree {
   void export_neighbors(int* col27, int* coarse8) const;
   void export_sorted_order(long* orig_of_sorted) const;
   void export_positions(double* r_orig_order) const;
+  // current positions [3n] and charges [n] in original order into device buffers (stream-ordered)
+  void gather_device(double* d_r, double* d_q) const;
+  long n_particles() const { return N_; }
+  int n_per_leaf() const { return n_per_leaf_; }
+  int digits() const { return digits_; }
+  const TreeOptions& options() const { return opt_; }
+  double box() const { return L_; }
   void export_pw(long node, int which, double* out) const;
   void export_W(double* out) const;
   void export_D(int level, double* out) const;

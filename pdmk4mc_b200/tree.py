@@ -91,6 +91,8 @@ def load_library():
                                          ctypes.c_void_p, ctypes.c_void_p]
     L.hpdmk_get_stream.restype = ctypes.c_int
     L.hpdmk_get_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    L.hpdmk_tree_rebuild.restype = ctypes.c_int
+    L.hpdmk_tree_rebuild.argtypes = [ctypes.c_void_p]
     L.hpdmk_ewald_energy.restype = ctypes.c_int
     L.hpdmk_ewald_energy.argtypes = [ctypes.c_void_p, _dp, _dp]
     L.hpdmk_set_mc_mode.restype = ctypes.c_int
@@ -199,8 +201,11 @@ class HPDMKPtTree:
             _check(L.hpdmk_last_error())
         self.n = int(n)
         self.L = float(params.L)
+        self._refresh_info()
+
+    def _refresh_info(self):
         info = np.zeros(5, np.int64)
-        _check(L.hpdmk_tree_info(self._h, _p(info, _lp)))
+        _check(load_library().hpdmk_tree_info(self._h, _p(info, _lp)))
         self.max_depth, self.n_nodes, _, self.dims_window, self.dims_diff = (int(v) for v in info)
 
     def close(self):
@@ -296,6 +301,11 @@ class HPDMKPtTree:
 
     def set_timing(self, on: bool):
         _check(load_library().hpdmk_set_timing(self._h, 1 if on else 0))
+
+    def rebuild(self):
+        """Re-bin the tree from the current positions and re-form the expansions."""
+        _check(load_library().hpdmk_tree_rebuild(self._h))
+        self._refresh_info()
 
     def ewald_energy(self):
         """FP64 Ewald energy of the current particles and its (real, reciprocal, self) parts."""

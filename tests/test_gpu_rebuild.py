@@ -1,0 +1,61 @@
+"""Tree maintenance: after many accepted moves (leaves drift from n_per_leaf
+and arrivals overflow into the pool), hpdmk_tree_rebuild re-bins the tree on
+the device. The rebuilt tree must equal a tree built from the current
+positions: the same nodes, neighbour lists and particle order, the same
+energies and energy shifts, and the same Metropolis run afterwards."""
+import numpy as np
+import pytest
+
+import pdmk4mc_b200 as P
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("mode", [P.MC_PERSISTENT, P.MC_GRAPH])
+def test_rebuild_equals_fresh_tree(mode):
+    n, L, npl, digits = 4000, 16.0, 10, 9
+    rng = np.random.default_rng(12)
+    c = rng.uniform(0, L, (4, 3))
+    r = np.mod(c[rng.integers(0, 4, n)] + rng.normal(0, L / 10, (n, 3)), L)
+    r[r >= L] = 0.0
+    r = np.ascontiguousarray(r.reshape(-1))
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    params = P.HPDMKParams(n_per_leaf=npl, digits=digits, L=L, init=P.DIRECT)
+    t = P.HPDMKPtTree(params, r, q, leaf_slack=1, pool_capacity=4096)
+    t.set_mc_mode(mode)
+    t.form_outgoing_pw()
+    t.form_incoming_pw()
+    m = 800
+    idx = rng.integers(0, n, m)
+    disp = rng.uniform(-1.5, 1.5, (m, 3))
+    u = rng.uniform(0, 1, m)
+    _, acc = t.mc_run(idx, disp, u, 0.05)  # hot: most moves accepted
+    assert acc.mean() > 0.5
+    t.rebuild()
+    pos = np.ascontiguousarray(t.positions())
+    f = P.HPDMKPtTree(params, pos, q, leaf_slack=1, pool_capacity=4096)
+    f.set_mc_mode(mode)
+    f.form_outgoing_pw()
+    f.form_incoming_pw()
+    try:
+        assert (t.max_depth, t.n_nodes) == (f.max_depth, f.n_nodes)
+        for a, b in zip(t.tree_nodes(), f.tree_nodes()):
+            np.testing.assert_array_equal(a, b)
+        for a, b in zip(t.tree_neighbors(), f.tree_neighbors()):
+            np.testing.assert_array_equal(a, b)
+        np.testing.assert_array_equal(t.sorted_order(), f.sorted_order())
+        np.testing.assert_array_equal(t.eval_energy_parts(), f.eval_energy_parts())
+        i2 = rng.integers(0, n, 64)
+        d2 = rng.uniform(-0.5, 0.5, (64, 3))
+        np.testing.assert_array_equal(t.eval_shift_energy_batch(i2, d2), f.eval_shift_energy_batch(i2, d2))
+        i3 = rng.integers(0, n, 200)
+        d3 = rng.uniform(-0.5, 0.5, (200, 3))
+        u3 = rng.uniform(0, 1, 200)
+        dt, at = t.mc_run(i3, d3, u3, 1.0)
+        df, af = f.mc_run(i3, d3, u3, 1.0)
+        np.testing.assert_array_equal(dt, df)
+        np.testing.assert_array_equal(at, af)
+        np.testing.assert_array_equal(t.positions(), f.positions())
+    finally:
+        t.close()
+        f.close()
