@@ -154,6 +154,20 @@ int hpdmk_eval_shift_energy_batch_static(hpdmk_tree tree, int m, const long *i, 
 int hpdmk_mc_run(hpdmk_tree tree, int n, const long *i, const double *d, const double *u, double beta, double *dE,
                  int *accepted);
 
+/* Replica sets (no reference counterpart): the Metropolis sequences of
+ * n_trees independent trees (same digits setting, same device) in one
+ * launch, one thread block per tree. Tree t runs moves c = 0 .. m-1 taken
+ * from i[t m + c], d[3 (t m + c) ..], u[t m + c]; outputs dE and accepted
+ * (either may be NULL) in the same layout. Same results as hpdmk_mc_run on
+ * each tree, to rounding. Host arrays. */
+int hpdmk_replicas_mc_run(int n_trees, const hpdmk_tree *trees, int m, const long *i, const double *d,
+                          const double *u, double beta, double *dE, int *accepted);
+
+/* Replica sets: form_outgoing_pw + form_incoming_pw + eval_energy of each
+ * tree, energy[t], with several trees in flight at once (each on its own
+ * stream, driven by a pool of host threads). No reference counterpart. */
+int hpdmk_replicas_energy(int n_trees, const hpdmk_tree *trees, double *energy);
+
 /* How hpdmk_mc_run / hpdmk_mc_run_device execute the sequence (no reference
  * counterpart): HPDMK_MC_PERSISTENT (default) runs it as one cooperative
  * launch on every SM with grid barriers between the phases of a move;

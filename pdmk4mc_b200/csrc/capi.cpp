@@ -4,12 +4,14 @@
 // include/utils.hpp:47, src/upward_pass.cpp:13).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/hpdmk.h"
@@ -391,6 +393,80 @@ int hpdmk_get_timing(hpdmk_tree t, double* out, int reset) {
     H(t)->tree->get_timing(out, reset != 0);
     return ok();
   });
+}
+
+int hpdmk_replicas_mc_run(int n_trees, const hpdmk_tree* trees, int m, const long* i, const double* d,
+                          const double* u, double beta, double* dE, int* accepted) {
+  if (n_trees < 1 || !trees || m < 0 || (m > 0 && (!i || !d || !u)))
+    return fail(HPDMK_ERR_BAD_INPUT, "bad replica arguments");
+  std::vector<pdmk::DmkTree*> ts;
+  for (int t = 0; t < n_trees; ++t) {
+    if (!trees[t]) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+    Handle* h = H(trees[t]);
+    if (h->device != H(trees[0])->device) return fail(HPDMK_ERR_BAD_INPUT, "replicas must share one device");
+    for (int c = 0; c < m; ++c) {
+      const size_t k = size_t(t) * m + c;
+      if (check_move(h, i[k], d[3 * k], d[3 * k + 1], d[3 * k + 2]) != HPDMK_OK) return g_last_error;
+    }
+    ts.push_back(h->tree.get());
+  }
+  if (m == 0) return ok();
+  Handle* h0 = H(trees[0]);
+  return guarded([&]() {
+    const size_t tot = size_t(n_trees) * m;
+    std::vector<int> ii(i, i + tot);
+    char* buf = nullptr;
+    const size_t bytes = tot * (4 + 24 + 8 + 8 + 4) + 64;
+    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), bytes, h0->stream));
+    double* d_d = reinterpret_cast<double*>(buf);
+    double* d_u = d_d + 3 * tot;
+    double* d_dE = d_u + tot;
+    int* d_i = reinterpret_cast<int*>(d_dE + tot);
+    int* d_acc = d_i + tot;
+    PDMK_CUDA(cudaMemcpyAsync(d_i, ii.data(), sizeof(int) * tot, cudaMemcpyHostToDevice, h0->stream));
+    PDMK_CUDA(cudaMemcpyAsync(d_d, d, sizeof(double) * 3 * tot, cudaMemcpyHostToDevice, h0->stream));
+    PDMK_CUDA(cudaMemcpyAsync(d_u, u, sizeof(double) * tot, cudaMemcpyHostToDevice, h0->stream));
+    for (auto* t : ts) t->reset_work();
+    pdmk::DmkTree::replicas_mc_run(ts, m, d_i, d_d, d_u, beta, d_dE, d_acc);
+    if (dE) PDMK_CUDA(cudaMemcpyAsync(dE, d_dE, sizeof(double) * tot, cudaMemcpyDeviceToHost, h0->stream));
+    if (accepted) PDMK_CUDA(cudaMemcpyAsync(accepted, d_acc, sizeof(int) * tot, cudaMemcpyDeviceToHost, h0->stream));
+    PDMK_CUDA(cudaFreeAsync(buf, h0->stream));
+    PDMK_CUDA(cudaStreamSynchronize(h0->stream));
+    for (int t = 0; t < n_trees; ++t)
+      if (int e = ts[t]->check_device_error()) return device_fail(e);
+    return ok();
+  });
+}
+
+int hpdmk_replicas_energy(int n_trees, const hpdmk_tree* trees, double* energy) {
+  if (n_trees < 1 || !trees || !energy) return fail(HPDMK_ERR_BAD_INPUT, "bad replica arguments");
+  for (int t = 0; t < n_trees; ++t)
+    if (!trees[t]) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  // each tree runs on its own stream; host threads keep several trees' work
+  // in flight, since every tree's pipeline waits on the device a few times
+  const int nth = std::max(1, std::min(n_trees, 16));
+  std::atomic<int> next{0};
+  std::vector<int> codes(n_trees, HPDMK_OK);
+  std::vector<std::string> msgs(n_trees);
+  std::vector<std::thread> pool;
+  for (int w = 0; w < nth; ++w)
+    pool.emplace_back([&]() {
+      for (int t = next++; t < n_trees; t = next++) {
+        Handle* h = H(trees[t]);
+        codes[t] = guarded([&]() {
+          PDMK_CUDA(cudaSetDevice(h->device));
+          h->tree->form_outgoing_pw();
+          h->tree->form_incoming_pw();
+          energy[t] = h->tree->eval_energy().total();
+          return ok();
+        });
+        if (codes[t] != HPDMK_OK) msgs[t] = g_last_message;
+      }
+    });
+  for (auto& th : pool) th.join();
+  for (int t = 0; t < n_trees; ++t)
+    if (codes[t] != HPDMK_OK) return fail(codes[t], "replica " + std::to_string(t) + ": " + msgs[t]);
+  return ok();
 }
 
 int hpdmk_tree_rebuild(hpdmk_tree t) {

@@ -1231,6 +1231,176 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Replica sets: the Metropolis sequences of many independent trees in one
+// launch, one thread block per tree (the block resolves, sums, decides,
+// updates and commits its tree's moves with block barriers only). Small
+// replicas do not need a whole GPU per move, so running them side by side
+// fills the SMs with independent work.
+constexpr int REP_T = 256;
+
+template <int NP>
+__global__ void __launch_bounds__(REP_T, 2) k_mc_rep(const DevTree* __restrict__ trees, int m, const int* __restrict__ idx,
+                                                  const double* __restrict__ disp, const double* __restrict__ u,
+                                                  double beta, double* __restrict__ dE_out, int* __restrict__ acc_out) {
+  extern __shared__ double2 sm2[];
+  __shared__ __align__(16) unsigned char ts_raw[sizeof(DevTree)];
+  __shared__ Header h;
+  __shared__ double red[4][32];
+  __shared__ double c_level[MAXLV + 2];
+  __shared__ Receiver rs[MAX_RECV];
+  __shared__ Proposal P;
+  __shared__ int s_acc;
+  {
+    const unsigned* src = reinterpret_cast<const unsigned*>(trees + blockIdx.x);
+    unsigned* dst = reinterpret_cast<unsigned*>(ts_raw);
+    for (int i = threadIdx.x; i < int(sizeof(DevTree) / 4); i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const DevTree& T = *reinterpret_cast<const DevTree*>(ts_raw);
+  const ResidualPoly<NP> poly(T);
+  const double pi = 3.14159265358979323846;
+  if (threadIdx.x >= 2 && threadIdx.x < MAXLV + 2) {
+    const double dk = level_dk(T, threadIdx.x);
+    c_level[threadIdx.x] = dk * dk * dk / (8.0 * pi * pi * pi) * level_dscale(threadIdx.x);
+  }
+  const double dk0 = T.delta_k[0];
+  const double c_window = dk0 * dk0 * dk0 / (8.0 * pi * pi * pi);
+  for (int mv = 0; mv < m; ++mv) {
+    const size_t c = size_t(blockIdx.x) * m + mv;
+    resolve(T, idx[c], disp + 3 * c, h);
+    const int lo_max = h.depth_o - 2, lt_max = h.depth_t - 2;
+    const int uo = min(h.depth_o - 1, T.pw_hi), ut = min(h.depth_t - 1, T.pw_hi);
+    const int per = 3 * (2 * T.n_window + 1) + max(max(uo, ut) - 1, 0) * 3 * (2 * T.n_diff + 1);
+    Tables to, oo;
+    alloc_tables(sm2, T, oo);
+    alloc_tables(sm2 + per, T, to);
+    build_tables(T, h.xo, h.q, h.Xo, uo, oo, threadIdx.x, blockDim.x);
+    build_tables(T, h.xt, h.q, h.Xt, ut, to, threadIdx.x, blockDim.x);
+    __syncthreads();
+    double acc[4] = {0, 0, 0, 0};
+    for (int k = threadIdx.x; k < T.Hw; k += blockDim.x) {
+      const double2 t = phase_at(to.root, k, T.dw), o = phase_at(oo.root, k, T.dw);
+      const double2 g = T.out_root[k];
+      const double ar = t.x - o.x, ai = t.y - o.y, br = g.x - o.x, bi = g.y - o.y;
+      acc[0] += (ar * br + ai * bi) * T.W[k];
+    }
+    const int base = T.pw_base, d = T.dd, n = T.n_diff;
+    for (int k = threadIdx.x; k < T.H; k += blockDim.x) {
+      const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
+      double sd = 0;
+      for (int l = 2; l <= lo_max; ++l) {
+        const double2 o = cmul(oo.lev[l][2][iz], cmul(oo.lev[l][1][iy], oo.lev[l][0][ix]));
+        const double2 cc = T.inc[size_t(h.path_o[l] - base) * T.H + k];
+        sd -= (o.x * cc.x - o.y * cc.y - (o.x * o.x + o.y * o.y)) * c_level[l];
+      }
+      for (int l = 2; l <= lt_max; ++l) {
+        const double2 t = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
+        const double2 cc = T.inc[size_t(h.path_t[l] - base) * T.H + k];
+        sd += (t.x * cc.x - t.y * cc.y) * c_level[l];
+      }
+      acc[1] += sd * T.D2[k];
+    }
+    const int lt = h.depth_t - 1, lo = h.depth_o - 1;
+    acc[2] = residual_sum(T, poly, h.path_t[lt], lt, h.Xt[lt], h.xt);
+    __syncthreads();  // the second call reuses the source-list arrays of the first
+    acc[3] = residual_sum(T, poly, h.path_o[lo], lo, h.Xo[lo], h.xo);
+    block_sum4(acc, red);
+    if (threadIdx.x == 0) {
+      double self = 0;
+      if (h.dr != 0) self = poly(h.dr, level_box(T, 2)) * h.q * h.q;
+      const double dE = acc[0] * c_window + acc[1] + (acc[2] - acc[3]) * h.q - self;
+      const int accd = u[c] < exp(-beta * dE) ? 1 : 0;
+      s_acc = accd;
+      if (dE_out) dE_out[c] = dE;
+      if (acc_out) acc_out[c] = accd;
+    }
+    __syncthreads();
+    if (!s_acc) continue;
+    // accept-and-update (src/tree.cpp:447-597) by this block
+    const int nr = build_receivers(T, h, rs);
+    if (threadIdx.x == 0) {
+      P.i_orig = h.i_orig;
+      P.slot = h.slot;
+      P.q = h.q;
+      for (int a = 0; a < 3; ++a) {
+        P.xo[a] = h.xo[a];
+        P.xt[a] = h.xt[a];
+      }
+      P.depth_o = h.depth_o;
+      P.depth_t = h.depth_t;
+      for (int l = 0; l < MAXLV; ++l) {
+        P.path_o[l] = l < h.depth_o ? h.path_o[l] : -1;
+        P.path_t[l] = l < h.depth_t ? h.path_t[l] : -1;
+      }
+      P.accepted = 1;
+      P.valid = 1;
+      P.n_recv = nr;
+      atomicAdd(&T.work[0], 1ull);
+      atomicAdd(&T.work[1], 32ull * ((unsigned long long)T.Hw + (unsigned long long)nr * T.H));
+      commit_move(T, P);
+    }
+    for (int k = threadIdx.x; k < T.Hw; k += blockDim.x) {
+      const double2 t = phase_at(to.root, k, T.dw), o = phase_at(oo.root, k, T.dw);
+      T.out_root[k] = csub(cadd(T.out_root[k], t), o);
+    }
+    for (int k = threadIdx.x; k < T.H; k += blockDim.x) {
+      const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
+      const int a0 = ((ix - n) % 3 + 3) % 3, a1 = ((iy - n) % 3 + 3) % 3, a2 = ((iz - n) % 3 + 3) % 3;
+      int r = 0;
+      while (r < nr) {
+        const int l = rs[r].level;
+        int re = r + 1;
+        while (re < nr && rs[re].level == l) ++re;
+        const double2 pt0 = cmul(to.lev[l][2][iz], cmul(to.lev[l][1][iy], to.lev[l][0][ix]));
+        const double2 po0 = cmul(oo.lev[l][2][iz], cmul(oo.lev[l][1][iy], oo.lev[l][0][ix]));
+        const double2 pt1 = cmul(pt0, root6(-2)), pt2 = cmul(pt0, root6(-4));
+        const double2 po1 = cmul(po0, root6(-2)), po2 = cmul(po0, root6(-4));
+        const int two_l = (l & 1) ? 2 : 1;
+        for (; r < re; r += UPD_UNROLL) {
+          double2 v[UPD_UNROLL];
+          size_t off[UPD_UNROLL];
+#pragma unroll
+          for (int q = 0; q < UPD_UNROLL; ++q) {
+            if (r + q < re) {
+              const Receiver& R = rs[r + q];
+              off[q] = size_t(R.off) * T.H + k;
+              v[q] = R.is_out ? T.out[off[q]] : T.inc[off[q]];
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < UPD_UNROLL; ++q) {
+            if (r + q < re) {
+              const Receiver& R = rs[r + q];
+              // the exponent sum lies in [-12, 12]
+              const int et = ((a0 * R.ft[0] + a1 * R.ft[1] + a2 * R.ft[2]) * two_l + 12) % 3;
+              const int eo = ((a0 * R.fo[0] + a1 * R.fo[1] + a2 * R.fo[2]) * two_l + 12) % 3;
+              double2 del = make_double2(0.0, 0.0);
+              if (R.has_t) del = et == 0 ? pt0 : (et == 1 ? pt1 : pt2);
+              if (R.has_o) del = csub(del, eo == 0 ? po0 : (eo == 1 ? po1 : po2));
+              if (R.is_out) T.out[off[q]] = cadd(v[q], del);
+              else T.inc[off[q]] = make_double2(v[q].x + del.x, v[q].y - del.y);
+            }
+          }
+        }
+        r = re;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+using McRepKernel = void (*)(const DevTree*, int, const int*, const double*, const double*, double, double*, int*);
+McRepKernel mc_rep_kernel(int np) {
+  switch (np) {
+    case 7: return k_mc_rep<7>;
+    case 13: return k_mc_rep<13>;
+    case 19: return k_mc_rep<19>;
+    case 25: return k_mc_rep<25>;
+    default: throw std::invalid_argument("unsupported residual polynomial");
+  }
+}
+
 using McKernel = void (*)(DevTree, McArgs);
 McKernel mc_kernel(int np) {
   switch (np) {
@@ -1752,6 +1922,49 @@ void DmkTree::shift_batch_static(int m, const long* h_idx, const double* h_disp,
   PDMK_CUDA(cudaMemcpyAsync(h_dE, s_dE, sizeof(double) * m, cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaStreamSynchronize(st_));
   last_valid_ = false;
+}
+
+// Metropolis sequences of many trees in one launch (k_mc_rep), ordered after
+// all their streams' earlier work on the first tree's stream.
+void DmkTree::replicas_mc_run(const std::vector<DmkTree*>& ts, int m, const int* d_idx, const double* d_disp,
+                              const double* d_u, double beta, double* d_dE, int* d_acc) {
+  if (ts.empty() || m <= 0) return;
+  const int np = ts[0]->dev_.n_poly;
+  size_t smem = 0;
+  std::vector<DevTree> hd;
+  for (DmkTree* t : ts) {
+    if (t->dev_.n_poly != np) throw std::invalid_argument("replicas must share the digits setting");
+    t->ensure_packed();
+    smem = std::max(smem, tables_smem(t->dev_, t->dev_.max_depth, 2));
+    hd.push_back(t->dev_);
+  }
+  cudaStream_t st = ts[0]->st_;
+  std::vector<cudaEvent_t> evs(ts.size());
+  for (auto& e : evs) PDMK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (size_t i = 1; i < ts.size(); ++i) {
+    PDMK_CUDA(cudaEventRecord(evs[i], ts[i]->st_));
+    PDMK_CUDA(cudaStreamWaitEvent(st, evs[i], 0));
+  }
+  DevTree* d_trees = nullptr;
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_trees), sizeof(DevTree) * hd.size(), st));
+  PDMK_CUDA(cudaMemcpyAsync(d_trees, hd.data(), sizeof(DevTree) * hd.size(), cudaMemcpyHostToDevice, st));
+  const McRepKernel kern = mc_rep_kernel(np);
+  static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function
+  const int slot = (np - 7) / 6;
+  if (smem > smem_set[slot]) {
+    PDMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    smem_set[slot] = smem;
+  }
+  kern<<<unsigned(ts.size()), REP_T, smem, st>>>(d_trees, m, d_idx, d_disp, d_u, beta, d_dE, d_acc);
+  PDMK_LAUNCH_CHECK();
+  PDMK_CUDA(cudaFreeAsync(d_trees, st));
+  PDMK_CUDA(cudaEventRecord(evs[0], st));
+  for (size_t i = 1; i < ts.size(); ++i) PDMK_CUDA(cudaStreamWaitEvent(ts[i]->st_, evs[0], 0));
+  for (auto& e : evs) PDMK_CUDA(cudaEventDestroy(e));  // released once the waits resolve
+  for (DmkTree* t : ts) {
+    t->last_valid_ = false;
+    t->diff_cached_ = false;
+  }
 }
 
 }  // namespace pdmk

@@ -190,6 +190,11 @@ class DmkTree {
   // Metropolis sequence mode: 0 one persistent cooperative launch (default),
   // 1 CUDA graphs of kGraphMoves (shift, update) launch pairs
   void set_mc_mode(int mode) { mc_mode_ = mode; }
+  // Metropolis sequences of m moves for each of many trees (same digits, same
+  // device) in one launch, one block per tree; arrays hold tree t's moves at
+  // [t m, (t + 1) m)
+  static void replicas_mc_run(const std::vector<DmkTree*>& trees, int m, const int* d_idx, const double* d_disp,
+                              const double* d_u, double beta, double* d_dE, int* d_acc);
   int mc_mode() const { return mc_mode_; }
   // batched energy shifts of many candidates against the current state
   void shift_batch_device(int m, const int* d_idx, const double* d_disp, double* d_dE);

@@ -71,6 +71,31 @@ def launch_count() -> int:
     return int(v.value)
 
 
+def replicas_mc_run(trees, idx, disp, u, beta):
+    """Metropolis sequences of many trees in one launch (one block per tree).
+    idx, u: [n_trees, m]; disp: [n_trees, m, 3]. Returns (dE, accepted), [n_trees, m]."""
+    nt = len(trees)
+    idx = np.ascontiguousarray(idx, dtype=np.int64).reshape(nt, -1)
+    m = idx.shape[1]
+    disp = np.ascontiguousarray(disp, dtype=np.float64).reshape(nt * m * 3)
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(nt * m)
+    hs = (ctypes.c_void_p * nt)(*[t._h for t in trees])
+    dE = np.zeros(nt * m)
+    acc = np.zeros(nt * m, np.int32)
+    _check(load_library().hpdmk_replicas_mc_run(nt, hs, m, _p(idx, _lp), _p(disp), _p(u), float(beta), _p(dE),
+                                                _p(acc, _ip)))
+    return dE.reshape(nt, m), acc.reshape(nt, m)
+
+
+def replicas_energy(trees):
+    """Full energy (outgoing, incoming, energy) of each tree, several in flight at once."""
+    nt = len(trees)
+    hs = (ctypes.c_void_p * nt)(*[t._h for t in trees])
+    e = np.zeros(nt)
+    _check(load_library().hpdmk_replicas_energy(nt, hs, _p(e)))
+    return e
+
+
 def load_library():
     global _LIB
     if _LIB is not None:
@@ -91,6 +116,11 @@ def load_library():
                                          ctypes.c_void_p, ctypes.c_void_p]
     L.hpdmk_get_stream.restype = ctypes.c_int
     L.hpdmk_get_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    L.hpdmk_replicas_mc_run.restype = ctypes.c_int
+    L.hpdmk_replicas_mc_run.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, _lp, _dp, _dp,
+                                        ctypes.c_double, _dp, _ip]
+    L.hpdmk_replicas_energy.restype = ctypes.c_int
+    L.hpdmk_replicas_energy.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), _dp]
     L.hpdmk_tree_rebuild.restype = ctypes.c_int
     L.hpdmk_tree_rebuild.argtypes = [ctypes.c_void_p]
     L.hpdmk_ewald_energy.restype = ctypes.c_int
