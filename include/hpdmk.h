@@ -182,6 +182,14 @@ int hpdmk_set_mc_mode(hpdmk_tree tree, int mode);
 int hpdmk_mc_run_device(hpdmk_tree tree, int n, const int *d_i, const double *d_d, const double *d_u, double beta,
                         double *d_dE, int *d_accepted);
 
+/* Potentials and fields (no counterpart in the reference, which evaluates
+ * energies only): phi[c] = dE/dq at particle i[c], the potential of all other
+ * particles and of the periodic images of all particles including its own,
+ * so that E = 1/2 sum_i q_i phi_i; field[3c..3c+2] = -grad phi there (may be
+ * NULL; the force on the particle is its charge times the field). The same
+ * expansions and near field as an energy shift; one launch for all m. */
+int hpdmk_eval_potential(hpdmk_tree tree, int m, const long *i, double *phi, double *field);
+
 /* Tree maintenance (no counterpart in the reference, which keeps the tree
  * built at construction and patches only its two lowest levels on moves,
  * src/tree.cpp:583-596): rebuild the octree, its neighbour lists and the

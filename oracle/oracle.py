@@ -115,6 +115,16 @@ def ewald_energy(L, r, q, s=5.0, alpha=1.0, nthreads=None):
     return lib().or_ewald_energy(L, s, alpha, len(q), _p(r), _p(q), nthreads or os.cpu_count())
 
 
+def ewald_potential(L, r, q, i, x, s=5.0, alpha=1.0, nthreads=None):
+    """Ewald potential at point x of all particles except i (src/ewald.cpp:281-308,
+    compute_potential, with particle i left out)."""
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    x = np.asarray(x, dtype=np.float64)
+    return lib().or_ewald_potential(L, s, alpha, len(q), _p(r), _p(q), x[0], x[1], x[2], int(i),
+                                    nthreads or os.cpu_count())
+
+
 def ewald_shift(L, r, q, i, d, s=5.0, alpha=1.0, nthreads=None):
     """Exact Ewald energy change of moving particle i by d (wrapped into the box):
     q_i [phi_{-i}(new) - phi_{-i}(old)]."""

@@ -395,6 +395,29 @@ int hpdmk_get_timing(hpdmk_tree t, double* out, int reset) {
   });
 }
 
+int hpdmk_eval_potential(hpdmk_tree t, int m, const long* i, double* phi, double* field) {
+  if (!t || m < 0 || (m > 0 && (!i || !phi))) return fail(HPDMK_ERR_BAD_INPUT, "bad potential arguments");
+  Handle* h = H(t);
+  for (int c = 0; c < m; ++c)
+    if (i[c] < 0 || i[c] >= h->n) return fail(HPDMK_ERR_BAD_INPUT, "particle index out of range");
+  if (m == 0) return ok();
+  return guarded([&]() {
+    h->ensure(m);
+    std::vector<int> ii(i, i + m);
+    double* d_field = nullptr;
+    if (field) PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_field), sizeof(double) * 3 * m, h->stream));
+    PDMK_CUDA(cudaMemcpyAsync(h->d_i, ii.data(), sizeof(int) * m, cudaMemcpyHostToDevice, h->stream));
+    h->tree->potential_batch(m, h->d_i, h->d_dE, d_field);
+    PDMK_CUDA(cudaMemcpyAsync(phi, h->d_dE, sizeof(double) * m, cudaMemcpyDeviceToHost, h->stream));
+    if (field) {
+      PDMK_CUDA(cudaMemcpyAsync(field, d_field, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, h->stream));
+      PDMK_CUDA(cudaFreeAsync(d_field, h->stream));
+    }
+    PDMK_CUDA(cudaStreamSynchronize(h->stream));
+    return ok();
+  });
+}
+
 int hpdmk_replicas_mc_run(int n_trees, const hpdmk_tree* trees, int m, const long* i, const double* d,
                           const double* u, double beta, double* dE, int* accepted) {
   if (n_trees < 1 || !trees || m < 0 || (m > 0 && (!i || !d || !u)))

@@ -1491,6 +1491,181 @@ ShiftBatchKernel shift_batch_kernel(int np) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Potential and field at particles (one block per particle): the same terms
+// as an energy shift, for the particle's own position only. With unit-charge
+// phases u(k) = exp(-i k.x) and the particle's charge q, the interaction with
+// all other particles is
+//   c_w sum_{k != 0} W Re(u conj(g - q u)) + sum_l c_l sum_k D (Re(u inc_l) - q |u|^2)
+//       + sum_{j != i} q_j res(r_ij),
+// and the returned potential adds 2 q C, C the particle's self terms of the
+// energy (window: c_w/2 sum W - psi0(0)/(2 bs_2 C0); each difference level on
+// its path: c_l/2 sum D_l - S_l), so that E = 1/2 sum_i q_i phi_i and
+// phi_i = dE/dq_i. The field is -grad phi, each plane wave differentiating to
+// -i k u.
+template <int NP>
+__global__ void __launch_bounds__(SB_T) k_potential_batch(DevTree T, const int* __restrict__ idx, double c_window,
+                                                          double self_w, const double* __restrict__ Sl,
+                                                          double* __restrict__ phi_out, double* __restrict__ field_out) {
+  extern __shared__ double2 sm2[];
+  __shared__ Header h;
+  __shared__ double red[4][32];
+  __shared__ double c_level[MAXLV + 2];
+  const ResidualPoly<NP> poly(T);
+  if (threadIdx.x >= 2 && threadIdx.x < MAXLV + 2) {
+    const double dk = level_dk(T, threadIdx.x);
+    c_level[threadIdx.x] = dk * dk * dk / (8.0 * 3.14159265358979323846 * 3.14159265358979323846 *
+                                           3.14159265358979323846) * level_dscale(threadIdx.x);
+  }
+  const int c = blockIdx.x;
+  const double zero3[3] = {0.0, 0.0, 0.0};
+  resolve(T, idx[c], zero3, h);
+  const int lo_max = h.depth_o - 2;
+  Tables uu;
+  alloc_tables(sm2, T, uu);
+  build_tables(T, h.xo, 1.0, h.Xo, lo_max, uu, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const double q = h.q;
+  double v[4] = {0, 0, 0, 0};   // window, difference, residual
+  double gw[4] = {0, 0, 0, 0};  // gradient of the window term
+  double gd[4] = {0, 0, 0, 0};  // gradient of the difference terms
+  double sums[4] = {0, 0, 0, 0};  // sum_{k != 0} W, sum D_2
+  {
+    const int dw = T.dw, nw = T.n_window;
+    const double dk0 = T.delta_k[0];
+    // the k = 0 mode is left out, as in Ewald summation: a neutral system has
+    // g(0) = 0, but all particles but one carry the net charge -q, whose
+    // k = 0 term is the uniform neutralising background's business
+    const int k_zero = (nw * dw + nw) * dw + nw;
+    for (int k = threadIdx.x; k < T.Hw; k += blockDim.x) {
+      if (k == k_zero) continue;
+      const double2 u = phase_at(uu.root, k, dw);
+      const double2 g = T.out_root[k];
+      const double bx = g.x - q * u.x, by = g.y - q * u.y;
+      const double w = T.W[k];
+      sums[0] += w;
+      v[0] += (u.x * bx + u.y * by) * w;
+      const double im = (u.y * bx - u.x * by) * w;  // Im(u conj(b))
+      const int ix = k % dw, iy = (k / dw) % dw, iz = k / (dw * dw);
+      gw[0] += dk0 * (ix - nw) * im;
+      gw[1] += dk0 * (iy - nw) * im;
+      gw[2] += dk0 * (iz - nw) * im;
+    }
+  }
+  {
+    const int base = T.pw_base, d = T.dd, n = T.n_diff;
+    for (int k = threadIdx.x; k < T.H; k += blockDim.x) {
+      const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
+      const double dd2 = T.D2[k];
+      sums[1] += dd2;
+      for (int l = 2; l <= lo_max; ++l) {
+        const double2 u = cmul(uu.lev[l][2][iz], cmul(uu.lev[l][1][iy], uu.lev[l][0][ix]));
+        const double2 cc = T.inc[size_t(h.path_o[l] - base) * T.H + k];
+        const double f = c_level[l] * dd2;
+        v[1] += (u.x * cc.x - u.y * cc.y - q * (u.x * u.x + u.y * u.y)) * f;
+        const double im = (u.x * cc.y + u.y * cc.x) * f;  // Im(u cc)
+        const double dkl = level_dk(T, l);
+        gd[0] += dkl * (ix - n) * im;
+        gd[1] += dkl * (iy - n) * im;
+        gd[2] += dkl * (iz - n) * im;
+      }
+    }
+  }
+  // near field: the source lists of the particle's leaf, the particle itself excluded
+  double gr[3] = {0, 0, 0};
+  {
+    const int lv = h.depth_o - 1;
+    const int leaf = h.path_o[lv];
+    const double b = level_box(T, lv);
+    const double eps = 2.220446049250313e-16;
+    __shared__ int m_beg[36], m_pre[37];
+    __shared__ double m_off[36][3];
+    if (threadIdx.x < 36) {
+      const int src = threadIdx.x;
+      int j = -1;
+      if (src == 0) j = leaf;
+      else if (src <= 27) j = (src - 1 == 13) ? -1 : T.col27[size_t(leaf) * 27 + (src - 1)];
+      else j = T.coarse8[size_t(leaf) * 8 + (src - 28)];
+      int beg = 0, cnt = 0;
+      double off[3] = {0, 0, 0};
+      if (j >= 0) {
+        const int lj = T.node_level[j];
+        const unsigned long long pj = T.node_prefix[j];
+        beg = T.node_begin[j];
+        cnt = (T.node_child0[j] < 0 ? beg + T.leaf_count[j] : T.node_end[j]) - beg;
+        const double bj = level_box(T, lj);
+        const int Xj[3] = {int(compact3(pj)), int(compact3(pj >> 1)), int(compact3(pj >> 2))};
+        for (int a = 0; a < 3; ++a)
+          off[a] = -periodic_shift_d(center_of(T.L, lv, h.Xo[lv][a]), center_of(T.L, lj, Xj[a]), T.L, b, bj) * T.L;
+      }
+      m_beg[src] = beg;
+      m_pre[src] = cnt;
+      for (int a = 0; a < 3; ++a) m_off[src][a] = off[a];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int src = 0; src < 36; ++src) {
+        const int nn = m_pre[src];
+        m_pre[src] = acc;
+        acc += nn;
+      }
+      m_pre[36] = acc;
+    }
+    __syncthreads();
+    const int total = m_pre[36];
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int lo = 0, hi = 36;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (m_pre[mid] <= e) lo = mid;
+        else hi = mid;
+      }
+      const int s = m_beg[lo] + (e - m_pre[lo]);
+      const double dx = h.xo[0] - (T.sx[s] + m_off[lo][0]), dy = h.xo[1] - (T.sy[s] + m_off[lo][1]),
+                   dz = h.xo[2] - (T.sz[s] + m_off[lo][2]);
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 > eps && r2 < b * b) {
+        const double r = sqrt(r2), qj = T.sq[s];
+        v[2] += qj * poly(r, b);
+        const double g = qj * poly.deriv(r, b) / r;
+        gr[0] += g * dx;
+        gr[1] += g * dy;
+        gr[2] += g * dz;
+      }
+    }
+    // arrivals parked in the overflow pool that belong to a source's subtree
+    // are folded into the slots by the host before this kernel runs
+  }
+  double v4[4] = {v[0], v[1], v[2], 0.0};
+  block_sum4(v4, red);
+  double w4[4] = {gw[0], gw[1], gw[2], 0.0};
+  block_sum4(w4, red);
+  double d4[4] = {gd[0], gd[1], gd[2], 0.0};
+  block_sum4(d4, red);
+  double r4[4] = {gr[0], gr[1], gr[2], 0.0};
+  block_sum4(r4, red);
+  block_sum4(sums, red);
+  if (threadIdx.x == 0) {
+    double cself = 0.5 * c_window * sums[0] - self_w;
+    for (int l = 2; l <= lo_max; ++l) cself += 0.5 * c_level[l] * sums[1] - Sl[l];
+    phi_out[c] = v4[0] * c_window + v4[1] + v4[2] + 2.0 * q * cself;
+    if (field_out)
+      for (int a = 0; a < 3; ++a) field_out[3 * size_t(c) + a] = -(w4[a] * c_window + d4[a] + r4[a]);
+  }
+}
+
+using PotentialKernel = void (*)(DevTree, const int*, double, double, const double*, double*, double*);
+PotentialKernel potential_kernel(int np) {
+  switch (np) {
+    case 7: return k_potential_batch<7>;
+    case 13: return k_potential_batch<13>;
+    case 19: return k_potential_batch<19>;
+    case 25: return k_potential_batch<25>;
+    default: throw std::invalid_argument("unsupported residual polynomial");
+  }
+}
+
 // the shift kernel for a residual polynomial of np coefficients (3, 6, 9, 12 digits)
 using ShiftKernel = void (*)(DevTree, ShiftArgs);
 ShiftKernel shift_kernel(int np) {
@@ -1965,6 +2140,27 @@ void DmkTree::replicas_mc_run(const std::vector<DmkTree*>& ts, int m, const int*
     t->last_valid_ = false;
     t->diff_cached_ = false;
   }
+}
+
+// Potentials and fields at many particles in one launch (k_potential_batch).
+void DmkTree::potential_batch(int m, const int* d_idx, double* d_phi, double* d_field) {
+  DevTree& D = dev_;
+  if (m <= 0) return;
+  ensure_packed();  // the near-field source lists read the slots only
+  prepare_box_lists();  // the per-level self terms S_l
+  const size_t smem = tables_smem(D, D.max_depth, 1);
+  const PotentialKernel kern = potential_kernel(D.n_poly);
+  static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
+  const int slot = (D.n_poly - 7) / 6;
+  if (smem > smem_set[slot]) {
+    PDMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    smem_set[slot] = smem;
+  }
+  const double pi = 3.14159265358979323846;
+  const double c_window = std::pow(D.delta_k[0], 3) / std::pow(2 * pi, 3);
+  const double self_w = ps_.psi0_0 / (2 * D.boxsize[2] * ps_.C0);
+  kern<<<unsigned(m), SB_T, smem, st_>>>(D, d_idx, c_window, self_w, d_Sl_, d_phi, d_field);
+  PDMK_LAUNCH_CHECK();
 }
 
 }  // namespace pdmk

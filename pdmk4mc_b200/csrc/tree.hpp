@@ -150,6 +150,18 @@ struct ResidualPoly {
     for (int i = 0; i < NP; ++i) v = fma(v, xs, c[i]);
     return v / r;
   }
+  // d/dr of the residual kernel, P'(x) (2 / b) / r - P(x) / r^2 with x = 2 r / b - 1
+  __device__ double deriv(double r, double b) const {
+    const double xs = (r / b - 0.5) * 2.0;
+    if (fabs(xs) >= 1.0) return 0.0;
+    double v = 0, dv = 0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      dv = fma(dv, xs, v);
+      v = fma(v, xs, c[i]);
+    }
+    return (dv * (2.0 / b) - v / r) / r;
+  }
 };
 
 struct EnergyParts {
@@ -193,6 +205,9 @@ class DmkTree {
   // Metropolis sequences of m moves for each of many trees (same digits, same
   // device) in one launch, one block per tree; arrays hold tree t's moves at
   // [t m, (t + 1) m)
+  // potential phi_i = sum_{j != i, images} q_j / r_ij and field -grad phi at
+  // original particles d_idx[0..m) into d_phi[m] and d_field[3m] (may be null)
+  void potential_batch(int m, const int* d_idx, double* d_phi, double* d_field);
   static void replicas_mc_run(const std::vector<DmkTree*>& trees, int m, const int* d_idx, const double* d_disp,
                               const double* d_u, double beta, double* d_dE, int* d_acc);
   int mc_mode() const { return mc_mode_; }

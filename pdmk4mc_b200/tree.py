@@ -119,6 +119,8 @@ def load_library():
     L.hpdmk_replicas_mc_run.restype = ctypes.c_int
     L.hpdmk_replicas_mc_run.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, _lp, _dp, _dp,
                                         ctypes.c_double, _dp, _ip]
+    L.hpdmk_eval_potential.restype = ctypes.c_int
+    L.hpdmk_eval_potential.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp]
     L.hpdmk_replicas_energy.restype = ctypes.c_int
     L.hpdmk_replicas_energy.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), _dp]
     L.hpdmk_tree_rebuild.restype = ctypes.c_int
@@ -331,6 +333,15 @@ class HPDMKPtTree:
 
     def set_timing(self, on: bool):
         _check(load_library().hpdmk_set_timing(self._h, 1 if on else 0))
+
+    def potential(self, idx, field=True):
+        """phi = dE/dq at particles idx (E = 1/2 sum q phi) and the field -grad phi."""
+        idx = np.ascontiguousarray(idx, dtype=np.int64).reshape(-1)
+        phi = np.zeros(idx.size)
+        f = np.zeros(3 * idx.size) if field else None
+        _check(load_library().hpdmk_eval_potential(self._h, int(idx.size), _p(idx, _lp), _p(phi),
+                                                   _p(f) if field else None))
+        return (phi, f.reshape(-1, 3)) if field else phi
 
     def rebuild(self):
         """Re-bin the tree from the current positions and re-form the expansions."""
