@@ -12,6 +12,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 
 #include "common.cuh"
@@ -24,6 +27,26 @@ namespace {
 constexpr int TPB = 256;
 
 inline unsigned grid_for(long n, int tpb = TPB) { return unsigned(std::max<long>(1, (n + tpb - 1) / tpb)); }
+
+// Small host values reach the device as a kernel argument: a cudaMemcpyAsync
+// from pageable host memory would first wait for the stream to drain.
+struct SmallWords {
+  int n;
+  uint32_t w[256];
+};
+
+__global__ void k_put_words(uint32_t* dst, SmallWords v) {
+  for (int i = threadIdx.x; i < v.n; i += blockDim.x) dst[i] = v.w[i];
+}
+
+void put_small(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  SmallWords v;
+  if (bytes % 4 != 0 || bytes > sizeof(v.w)) throw std::logic_error("put_small: size");
+  v.n = int(bytes / 4);
+  std::memcpy(v.w, src, bytes);
+  k_put_words<<<1, 64, 0, st>>>(static_cast<uint32_t*>(dst), v);
+  PDMK_LAUNCH_CHECK();
+}
 
 // ---------------------------------------------------------------------------
 __global__ void k_keys(const double* r, long n, double L, uint64_t* key, int* val) {
@@ -99,29 +122,33 @@ __global__ void k_refine_level(const uint64_t* keys, long n, int level, int n_pe
 }
 
 // 2:1 balance: a refined cell at level k needs all 26 neighbours at level k
-// to exist, i.e. their parents (level k-1) and all ancestors refined.
-__global__ void k_balance_level(Bitmaps B, int level) {
-  long nwords = (1L << (3 * level)) >> 5;
-  if (nwords == 0) nwords = 1;
-  long w = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (w >= nwords) return;
-  uint32_t bits = B.bm[level][w];
+// to exist, i.e. their parents (level k-1) and all ancestors refined. One
+// thread per (cell, neighbour) pair where that fits in kBalanceFanThreads
+// threads, one thread per cell with a loop over its 26 neighbours on deeper,
+// larger levels. A walk up the ancestors stops at the first cell already
+// refined: a refined cell's ancestors are refined too, or are being set by the
+// thread that refined it, so the bitmaps at the end are the same union.
+constexpr long kBalanceFanThreads = 1L << 24;
+
+__global__ void k_balance_level(Bitmaps B, int level, int fan) {
+  const long ncells = 1L << (3 * level);
+  const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long cell = t / fan;
+  if (cell >= ncells || !bit_get(B.bm[level], uint64_t(cell))) return;
+  const int k0 = fan == 26 ? int(t % 26) : 0, k1 = fan == 26 ? k0 + 1 : 26;
   const uint32_t mask = (1u << level) - 1u;
-  while (bits) {
-    int b = __ffs(bits) - 1;
-    bits &= bits - 1;
-    uint64_t cell = (uint64_t(w) << 5) | uint64_t(b);
-    uint32_t X = compact3(cell), Y = compact3(cell >> 1), Z = compact3(cell >> 2);
-    for (int dz = -1; dz <= 1; ++dz)
-      for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx) {
-          if (!dx && !dy && !dz) continue;
-          uint64_t nb = morton3((X + dx) & mask, (Y + dy) & mask, (Z + dz) & mask);
-          for (int lv = level - 1; lv >= 0; --lv) {
-            nb >>= 3;
-            bit_set(B.bm[lv], nb);
-          }
-        }
+  const uint32_t X = compact3(uint64_t(cell)), Y = compact3(uint64_t(cell) >> 1), Z = compact3(uint64_t(cell) >> 2);
+  for (int k = k0; k < k1; ++k) {
+    const int j = k < 13 ? k : k + 1;  // 3x3x3 offsets without the centre (13)
+    const int dx = j % 3 - 1, dy = (j / 3) % 3 - 1, dz = j / 9 - 1;
+    uint64_t nb = morton3((X + dx) & mask, (Y + dy) & mask, (Z + dz) & mask);
+    for (int lv = level - 1; lv >= 0; --lv) {
+      nb >>= 3;
+      uint32_t* wp = B.bm[lv] + (nb >> 5);
+      const uint32_t m = 1u << (nb & 31);
+      if (*wp & m) break;
+      if (atomicOr(wp, m) & m) break;
+    }
   }
 }
 
@@ -516,13 +543,13 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
   PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&lists[0]), size_t(list_cap) * 8, st_));
   PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&lists[1]), size_t(list_cap) * 8, st_));
   uint64_t zero = 0;
-  PDMK_CUDA(cudaMemcpyAsync(lists[0], &zero, 8, cudaMemcpyHostToDevice, st_));
+  put_small(lists[0], &zero, 8, st_);
   int maxref = 0;  // deepest level holding a refined cell
   {
     // root: refined (all nodes above level 2 are refined)
     B.bm[0] = static_cast<uint32_t*>(alloc(4));
     uint32_t one = 1;
-    PDMK_CUDA(cudaMemcpyAsync(B.bm[0], &one, 4, cudaMemcpyHostToDevice, st_));
+    put_small(B.bm[0], &one, 4, st_);
     int n_par = 1;
     int cur = 0;
     for (int l = 1; l <= MAX_LEVEL; ++l) {
@@ -547,7 +574,9 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
   }
   // 2:1 balance, deepest refined level first
   for (int k = maxref; k >= 2; --k) {
-    k_balance_level<<<grid_for(nwords[k]), TPB, 0, st_>>>(B, k);
+    const long cells = 1L << (3 * k);
+    const int fan = cells * 26 <= kBalanceFanThreads ? 26 : 1;
+    k_balance_level<<<grid_for(cells * fan), TPB, 0, st_>>>(B, k, fan);
     PDMK_LAUNCH_CHECK();
   }
   // ranks of refined cells
@@ -576,11 +605,11 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
   D.n_nodes = n_nodes;
   for (int l = 0; l <= nlev && l < MAX_LEVELS + 2; ++l) D.level_start[l] = h_level_start_[l];
   int* d_level_start = static_cast<int*>(alloc(sizeof(int) * (nlev + 1)));
-  PDMK_CUDA(cudaMemcpyAsync(d_level_start, h_level_start_.data(), sizeof(int) * (nlev + 1), cudaMemcpyHostToDevice, st_));
+  put_small(d_level_start, h_level_start_.data(), sizeof(int) * (nlev + 1), st_);
   D.boxsize[0] = L_;
   for (int l = 1; l < MAX_LEVELS + 2; ++l) D.boxsize[l] = 0.5 * D.boxsize[l - 1];
   double* d_boxsize = static_cast<double*>(alloc(sizeof(double) * (MAX_LEVELS + 2)));
-  PDMK_CUDA(cudaMemcpyAsync(d_boxsize, D.boxsize, sizeof(double) * (MAX_LEVELS + 2), cudaMemcpyHostToDevice, st_));
+  put_small(d_boxsize, D.boxsize, sizeof(double) * (MAX_LEVELS + 2), st_);
 
   NodeArrays na;
   na.prefix = static_cast<uint64_t*>(alloc(sizeof(uint64_t) * n_nodes));
@@ -590,10 +619,10 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
   {
     uint64_t p0 = 0;
     int l0 = 0, par0 = -1, c0 = 1;
-    PDMK_CUDA(cudaMemcpyAsync(na.prefix, &p0, 8, cudaMemcpyHostToDevice, st_));
-    PDMK_CUDA(cudaMemcpyAsync(na.level, &l0, 4, cudaMemcpyHostToDevice, st_));
-    PDMK_CUDA(cudaMemcpyAsync(na.parent, &par0, 4, cudaMemcpyHostToDevice, st_));
-    PDMK_CUDA(cudaMemcpyAsync(na.child0, &c0, 4, cudaMemcpyHostToDevice, st_));
+    put_small(na.prefix, &p0, 8, st_);
+    put_small(na.level, &l0, 4, st_);
+    put_small(na.parent, &par0, 4, st_);
+    put_small(na.child0, &c0, 4, st_);
   }
   for (int l = 1; l < nlev; ++l) {
     k_enum_nodes<<<grid_for(nwords[l - 1]), TPB, 0, st_>>>(B, l, maxref, d_level_start, na);
@@ -612,7 +641,7 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
       ptrs[MAX_LEVELS + l] = D.wprefix[l];
     }
     void** d_ptrs = static_cast<void**>(alloc(sizeof(ptrs)));
-    PDMK_CUDA(cudaMemcpyAsync(d_ptrs, ptrs, sizeof(ptrs), cudaMemcpyHostToDevice, st_));
+    put_small(d_ptrs, ptrs, sizeof(ptrs), st_);
     D.bm_d = reinterpret_cast<const uint32_t* const*>(d_ptrs);
     D.wprefix_d = reinterpret_cast<const int* const*>(d_ptrs + MAX_LEVELS);
   }
@@ -703,7 +732,8 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
   D.err = D.pool_n + 1;
   D.work = reinterpret_cast<unsigned long long*>(D.pool_n + 4);
   PDMK_CUDA(cudaMemsetAsync(D.pool_n, 0, 64, st_));
-  PDMK_CUDA(cudaStreamSynchronize(st_));
+  // no synchronisation: the inputs were consumed before the refinement
+  // loop's first read-back, and everything after is stream-ordered
 }
 
 // Lay the particles of each DFS leaf j (dense source rows [src_lo[j],
@@ -721,11 +751,11 @@ void DmkTree::layout_slots(const double* dsx, const double* dsy, const double* d
     exclusive_scan(leaf_dev_.cnt, leaf_dev_.cnt_prefix, nl, scr, st_);
     PDMK_CUDA(cudaFreeAsync(scr, st_));
   }
-  int last_begin = 0, last_cap = 0;
-  PDMK_CUDA(cudaMemcpyAsync(&last_begin, begin + nl - 1, 4, cudaMemcpyDeviceToHost, st_));
-  PDMK_CUDA(cudaMemcpyAsync(&last_cap, leaf_dev_.cap + nl - 1, 4, cudaMemcpyDeviceToHost, st_));
-  PDMK_CUDA(cudaStreamSynchronize(st_));
-  const int n_slots = last_begin + last_cap;
+  // every particle sits in exactly one leaf and cap = cnt + slack, so the
+  // slots total N + nl * slack without a look at the device
+  const long n_slots_l = N_ + long(nl) * leaf_slack;
+  if (n_slots_l > std::numeric_limits<int>::max()) throw std::runtime_error("tree build: too many slots");
+  const int n_slots = int(n_slots_l);
   // captured graphs hold the tree description by value: rebuild them later
   for (auto& gx : mc_graph_)
     if (gx) {
@@ -811,6 +841,101 @@ void DmkTree::repack(int leaf_slack) {
 }
 
 // ---------------------------------------------------------------------------
+namespace {
+
+// Window table W (window_matrix, include/kernels.hpp:60-86) and the level-2
+// difference table D2 (difference_matrix, include/kernels.hpp:88-114; every
+// other level is D2 scaled by 4^-(l-2), since k sigma_l is level-free).
+//
+// An entry depends on its mode only through m = ix^2 + iy^2 + iz^2 (in units
+// of dk), and the transform arguments |k| sigma = sqrt(m) dk sigma do not
+// depend on L: dk sigma is pi / (2c) for the window (dk = 2 pi / L, sigma_2 =
+// L / 4c) and 2 pi / 3c, pi / 3c for the two difference terms (dk = 8 pi / 3L,
+// sigma_2, sigma_3 = L / 8c). So the psi_0 transforms, the costly part, are
+// evaluated once per digits setting and m; a table is those values over
+// k^2 = kx^2 + ky^2 + kz^2 of its L. Whole tables are also kept per
+// (digits, L) in pinned host memory (each tree's copy to the device is then
+// asynchronous and never reads freed memory); past kMaxCached pairs (a run
+// over many box sizes) they go to the caller's pageable `own` vector, whose
+// copies are staged before cudaMemcpyAsync returns. Both routes give the same
+// values.
+struct KernelTables {
+  const double* W = nullptr;
+  const double* D2 = nullptr;
+};
+
+struct ModeTransforms {
+  std::vector<double> w;  // F(sqrt(m) pi / 2c), m = 0 .. 3 nw^2
+  std::vector<double> d;  // F(sqrt(m) pi / 3c) - F(sqrt(m) 2 pi / 3c), m = 0 .. 3 nd^2
+};
+
+KernelTables kernel_tables(const ProlateSetup& s, double L, std::vector<double>& own) {
+  constexpr size_t kMaxCached = 32;
+  constexpr double pi = 3.14159265358979323846;
+  static std::mutex mu;
+  static std::map<int, ModeTransforms> transforms;
+  static std::map<std::pair<int, uint64_t>, KernelTables> cache;
+  uint64_t lbits;
+  std::memcpy(&lbits, &L, 8);
+  std::lock_guard<std::mutex> g(mu);
+  auto key = std::make_pair(s.digits, lbits);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  const int nw = s.n_window, dw = 2 * nw + 1, nd = s.n_diff, dd = 2 * nd + 1;
+  auto ft = transforms.find(s.digits);
+  if (ft == transforms.end()) {
+    ModeTransforms t;
+    t.w.resize(3 * nw * nw + 1);
+    t.d.resize(3 * nd * nd + 1);
+    for (size_t m = 1; m < t.w.size(); ++m) t.w[m] = s.fourier(std::sqrt(double(m)) * (pi / (2 * s.c)));
+    for (size_t m = 1; m < t.d.size(); ++m) {
+      const double r = std::sqrt(double(m));
+      t.d[m] = s.fourier(r * (pi / (3 * s.c))) - s.fourier(r * (2 * pi / (3 * s.c)));
+    }
+    ft = transforms.emplace(s.digits, std::move(t)).first;
+  }
+  const ModeTransforms& F = ft->second;
+  const size_t hw = size_t(dw) * dw * (nw + 1), hd = size_t(dd) * dd * (nd + 1);
+  double* W;
+  const bool cached = cache.size() < kMaxCached;
+  if (cached) {
+    PDMK_CUDA(cudaMallocHost(reinterpret_cast<void**>(&W), sizeof(double) * (hw + hd)));
+  } else {
+    own.resize(hw + hd);
+    W = own.data();
+  }
+  double* D2 = W + hw;
+  {
+    const double dk = 2 * pi / L;
+    for (int k = 0; k < nw + 1; ++k)
+      for (int j = 0; j < dw; ++j)
+        for (int i = 0; i < dw; ++i) {
+          const int m = (i - nw) * (i - nw) + (j - nw) * (j - nw) + (k - nw) * (k - nw);
+          const double kx = (i - nw) * dk, ky = (j - nw) * dk, kz = (k - nw) * dk;
+          const double k2 = kx * kx + ky * ky + kz * kz;
+          const double v = m != 0 ? F.w[m] / k2 : 0.0;
+          W[(k * dw + j) * dw + i] = (k == nw) ? v : 2 * v;
+        }
+  }
+  {
+    const double dk = (2 * pi / 3) / (0.25 * L), sl = 0.25 * L / s.c, slp1 = 0.5 * sl;
+    for (int k = 0; k < nd + 1; ++k)
+      for (int j = 0; j < dd; ++j)
+        for (int i = 0; i < dd; ++i) {
+          const int m = (i - nd) * (i - nd) + (j - nd) * (j - nd) + (k - nd) * (k - nd);
+          const double kx = (i - nd) * dk, ky = (j - nd) * dk, kz = (k - nd) * dk;
+          const double k2 = kx * kx + ky * ky + kz * kz;
+          const double v = m != 0 ? F.d[m] / k2 : s.diff0 * (slp1 * slp1 - sl * sl);
+          D2[(k * dd + j) * dd + i] = (k == nd) ? v : 2 * v;
+        }
+  }
+  KernelTables t{W, D2};
+  if (cached) cache.emplace(key, t);
+  return t;
+}
+
+}  // namespace
+
 void DmkTree::build_setup() {
   DevTree& D = dev_;
   const ProlateSetup& s = ps_;
@@ -824,63 +949,19 @@ void DmkTree::build_setup() {
   for (int i = 0; i < MAX_POLY; ++i) D.poly[i] = i < D.n_poly ? s.poly[i] : 0.0;
   const double pi = 3.14159265358979323846;
   // form_wavenumbers (src/tree.cpp:46-68)
-  std::vector<double> sig(MAX_LEVELS + 2);
-  sig[0] = L_ / s.c;
-  for (int l = 1; l < MAX_LEVELS + 2; ++l) sig[l] = 0.5 * sig[l - 1];
   D.delta_k[0] = D.delta_k[1] = 2 * pi / L_;
   for (int l = 2; l < MAX_LEVELS + 2; ++l) D.delta_k[l] = (2.0 * pi / 3.0) / D.boxsize[l];
   for (int l = 0; l < MAX_LEVELS + 2; ++l) D.dscale[l] = l >= 2 ? std::ldexp(1.0, -2 * (l - 2)) : 0.0;
   D.pw_lo = 2;
   D.pw_hi = D.max_depth - 2;  // may be < pw_lo: no difference levels
   D.pw_base = D.level_start[D.pw_lo];
-  // window_matrix (include/kernels.hpp:60-86)
-  // The kernels depend on a mode only through m = ix^2 + iy^2 + iz^2 (in units
-  // of dk), so psi_0 is evaluated once per distinct m.
-  std::vector<double> W(D.Hw);
-  {
-    int nk = s.n_window, d = D.dw;
-    double dk = D.delta_k[1], sigma = sig[2];
-    std::vector<double> memo(3 * nk * nk + 1, std::nan(""));
-    for (int k = 0; k < nk + 1; ++k)
-      for (int j = 0; j < d; ++j)
-        for (int i = 0; i < d; ++i) {
-          int m = (i - nk) * (i - nk) + (j - nk) * (j - nk) + (k - nk) * (k - nk);
-          if (std::isnan(memo[m])) {
-            double kx = (i - nk) * dk, ky = (j - nk) * dk, kz = (k - nk) * dk;
-            double k2 = kx * kx + ky * ky + kz * kz;
-            memo[m] = k2 != 0 ? s.fourier(std::sqrt(k2) * sigma) / k2 : 0.0;
-          }
-          W[(k * d + j) * d + i] = (k == nk) ? memo[m] : 2 * memo[m];
-        }
-  }
-  // difference_matrix at level 2 (include/kernels.hpp:88-114); every other
-  // level is this table scaled by 4^-(l-2), since k sigma_l is level-free
-  std::vector<double> D2(D.H);
-  {
-    int nk = s.n_diff, d = D.dd;
-    double dk = D.delta_k[2], sl = sig[2], slp1 = sig[3];
-    std::vector<double> memo(3 * nk * nk + 1, std::nan(""));
-    for (int k = 0; k < nk + 1; ++k)
-      for (int j = 0; j < d; ++j)
-        for (int i = 0; i < d; ++i) {
-          int m = (i - nk) * (i - nk) + (j - nk) * (j - nk) + (k - nk) * (k - nk);
-          if (std::isnan(memo[m])) {
-            double kx = (i - nk) * dk, ky = (j - nk) * dk, kz = (k - nk) * dk;
-            double k2 = kx * kx + ky * ky + kz * kz;
-            if (k2 == 0) {
-              memo[m] = s.diff0 * (slp1 * slp1 - sl * sl);
-            } else {
-              double kk = std::sqrt(k2);
-              memo[m] = (s.fourier(kk * slp1) - s.fourier(kk * sl)) / k2;
-            }
-          }
-          D2[(k * d + j) * d + i] = (k == nk) ? memo[m] : 2 * memo[m];
-        }
-  }
+  // window and difference tables, shared by every tree of this (digits, L)
+  std::vector<double> own;
+  const KernelTables kt = kernel_tables(s, L_, own);
   D.W = static_cast<double*>(alloc(sizeof(double) * D.Hw));
   D.D2 = static_cast<double*>(alloc(sizeof(double) * D.H));
-  PDMK_CUDA(cudaMemcpyAsync(D.W, W.data(), sizeof(double) * D.Hw, cudaMemcpyHostToDevice, st_));
-  PDMK_CUDA(cudaMemcpyAsync(D.D2, D2.data(), sizeof(double) * D.H, cudaMemcpyHostToDevice, st_));
+  PDMK_CUDA(cudaMemcpyAsync(D.W, kt.W, sizeof(double) * D.Hw, cudaMemcpyHostToDevice, st_));
+  PDMK_CUDA(cudaMemcpyAsync(D.D2, kt.D2, sizeof(double) * D.H, cudaMemcpyHostToDevice, st_));
   // expansions (src/tree.cpp:414-443)
   D.out_root = static_cast<double2*>(alloc(sizeof(double2) * D.Hw));
   PDMK_CUDA(cudaMemsetAsync(D.out_root, 0, sizeof(double2) * D.Hw, st_));
@@ -901,7 +982,6 @@ void DmkTree::build_setup() {
   d_one_idx_ = static_cast<int*>(alloc(64));
   d_one_disp_ = static_cast<double*>(alloc(64));
   d_one_u_ = static_cast<double*>(alloc(64));
-  PDMK_CUDA(cudaStreamSynchronize(st_));
 }
 
 int DmkTree::check_device_error() const {

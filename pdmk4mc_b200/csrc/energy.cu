@@ -14,6 +14,7 @@
 // so the decentring factor is an exact sixth root of unity per axis.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "common.cuh"
@@ -404,7 +405,9 @@ __global__ void k_diff_finish(DevTree T, const int* __restrict__ boxes, int nbox
   if (threadIdx.x == 0) *out = s;
 }
 
-__global__ void k_window(DevTree T, double scale, double self, double* out) {
+// window energy; the self term sum(q^2) psi_0(0) / (2 b_2 C0) takes sum(q^2)
+// from the device (q2) so that no host round trip is needed
+__global__ void k_window(DevTree T, double scale, const double* q2, double psi0_0, double self_den, double* out) {
   __shared__ double sm[32];
   double e = 0;
   for (int k = threadIdx.x; k < T.Hw; k += blockDim.x) {
@@ -412,7 +415,7 @@ __global__ void k_window(DevTree T, double scale, double self, double* out) {
     e += (o.x * o.x + o.y * o.y) * T.W[k];
   }
   double s = block_sum(e, sm);
-  if (threadIdx.x == 0) *out = s * scale - self;
+  if (threadIdx.x == 0) *out = s * scale - *q2 * psi0_0 / self_den;
 }
 
 
@@ -725,24 +728,34 @@ size_t DmkTree::partials_needed() const {
 }
 
 void DmkTree::ensure_packed() {
+  // only accepted moves put particles into the overflow pool: a tree without
+  // moves since its build or last pack needs no device round trip
+  if (!moved_) return;
   int pn = 0;
   PDMK_CUDA(cudaMemcpyAsync(&pn, dev_.pool_n, 4, cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaStreamSynchronize(st_));
   if (pn > 0) repack(opt_.leaf_slack);
+  moved_ = false;
 }
 
 void DmkTree::form_outgoing_pw() {
   ensure_packed();
   DevTree& D = dev_;
-  // host view of node slot ranges and coordinates for the work list
+  // host view of node slot ranges and coordinates for the work list (and, on
+  // a new tree, of the children for the box lists: one round trip for both)
   const int nn = D.n_nodes;
-  std::vector<int> nb(nn), ne(nn), lv(nn);
+  std::vector<int> nb(nn), ne(nn), lv(nn), c0;
   std::vector<uint64_t> pf(nn);
   PDMK_CUDA(cudaMemcpyAsync(nb.data(), D.node_begin, 4 * nn, cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaMemcpyAsync(ne.data(), D.node_end, 4 * nn, cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaMemcpyAsync(lv.data(), D.node_level, 4 * nn, cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaMemcpyAsync(pf.data(), D.node_prefix, 8 * nn, cudaMemcpyDeviceToHost, st_));
+  if (!box_lists_ready_) {
+    c0.resize(nn);
+    PDMK_CUDA(cudaMemcpyAsync(c0.data(), D.node_child0, 4 * nn, cudaMemcpyDeviceToHost, st_));
+  }
   PDMK_CUDA(cudaStreamSynchronize(st_));
+  if (!box_lists_ready_) build_box_lists(c0);
   struct Box {
     int node, sb, se, level;
     double2* out;
@@ -837,12 +850,33 @@ void DmkTree::form_outgoing_pw() {
       }
     }
   }
-  NudftWork* d_work;
-  size_t nw = wroot.size() + wbox.size();
-  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_work), sizeof(NudftWork) * (nw + 1), st_));
-  std::vector<NudftWork> all(wbox);
-  all.insert(all.end(), wroot.begin(), wroot.end());
-  PDMK_CUDA(cudaMemcpyAsync(d_work, all.data(), sizeof(NudftWork) * nw, cudaMemcpyHostToDevice, st_));
+  // one upload: the work items (boxes first, then the root chunks), then per
+  // split-K group its first chunk, chunk count and output, for the reductions
+  const size_t nw = wroot.size() + wbox.size();
+  auto align16 = [](size_t b) { return (b + 15) & ~size_t(15); };
+  const size_t off_rmeta = align16(sizeof(NudftWork) * nw);
+  const size_t off_rout = align16(off_rmeta + sizeof(int) * 2 * root_split.size());
+  const size_t off_bmeta = align16(off_rout + sizeof(double2*) * root_split.size());
+  const size_t off_bout = align16(off_bmeta + sizeof(int) * 2 * box_split.size());
+  const size_t blob_bytes = align16(off_bout + sizeof(double2*) * box_split.size()) + 16;
+  std::vector<unsigned char> blob(blob_bytes, 0);
+  std::memcpy(blob.data(), wbox.data(), sizeof(NudftWork) * wbox.size());
+  std::memcpy(blob.data() + sizeof(NudftWork) * wbox.size(), wroot.data(), sizeof(NudftWork) * wroot.size());
+  auto put_meta = [&](const std::vector<Chunked>& sp, size_t off_meta, size_t off_out) {
+    int* meta = reinterpret_cast<int*>(blob.data() + off_meta);
+    double2** outs = reinterpret_cast<double2**>(blob.data() + off_out);
+    for (size_t i = 0; i < sp.size(); ++i) {
+      meta[i] = sp[i].first;
+      meta[sp.size() + i] = sp[i].n;
+      outs[i] = sp[i].out;
+    }
+  };
+  put_meta(root_split, off_rmeta, off_rout);
+  put_meta(box_split, off_bmeta, off_bout);
+  unsigned char* d_blob;
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_blob), blob_bytes, st_));
+  PDMK_CUDA(cudaMemcpyAsync(d_blob, blob.data(), blob_bytes, cudaMemcpyHostToDevice, st_));
+  NudftWork* d_work = reinterpret_cast<NudftWork*>(d_blob);
   // the root pass (few CTAs) overlaps the box pass on a second stream
   if (!aux_) {
     PDMK_CUDA(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking));
@@ -858,42 +892,32 @@ void DmkTree::form_outgoing_pw() {
   time_end(3);
   PDMK_CUDA(cudaStreamWaitEvent(st_, ev_join_, 0));
   // reduce split-K chunks
-  auto reduce = [&](const std::vector<Chunked>& sp, const double2* pbase, int H) {
+  auto reduce = [&](const std::vector<Chunked>& sp, const double2* pbase, int H, size_t off_meta, size_t off_out) {
     if (sp.empty()) return;
-    int nbx = int(sp.size());
-    std::vector<int> first(nbx), cntv(nbx);
-    std::vector<double2*> outs(nbx);
-    for (int i = 0; i < nbx; ++i) {
-      first[i] = sp[i].first;
-      cntv[i] = sp[i].n;
-      outs[i] = sp[i].out;
-    }
-    int* d_meta;
-    double2** d_outs;
-    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_meta), sizeof(int) * 2 * nbx + 16, st_));
-    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_outs), sizeof(double2*) * nbx + 16, st_));
-    PDMK_CUDA(cudaMemcpyAsync(d_meta, first.data(), sizeof(int) * nbx, cudaMemcpyHostToDevice, st_));
-    PDMK_CUDA(cudaMemcpyAsync(d_meta + nbx, cntv.data(), sizeof(int) * nbx, cudaMemcpyHostToDevice, st_));
-    PDMK_CUDA(cudaMemcpyAsync(d_outs, outs.data(), sizeof(double2*) * nbx, cudaMemcpyHostToDevice, st_));
+    const int nbx = int(sp.size());
+    const int* d_meta = reinterpret_cast<const int*>(d_blob + off_meta);
+    double2* const* d_outs = reinterpret_cast<double2* const*>(d_blob + off_out);
     dim3 grid(grid_for(H), unsigned(nbx));
     k_reduce_chunks<<<grid, TPB, 0, st_>>>(pbase, d_meta, d_meta + nbx, d_outs, H);
     PDMK_LAUNCH_CHECK();
-    PDMK_CUDA(cudaFreeAsync(d_meta, st_));
-    PDMK_CUDA(cudaFreeAsync(d_outs, st_));
   };
-  reduce(root_split, part, D.Hw);
-  reduce(box_split, part_b, D.H);
-  PDMK_CUDA(cudaFreeAsync(d_work, st_));
+  reduce(root_split, part, D.Hw, off_rmeta, off_rout);
+  reduce(box_split, part_b, D.H, off_bmeta, off_bout);
+  PDMK_CUDA(cudaFreeAsync(d_blob, st_));
   PDMK_CUDA(cudaFreeAsync(part, st_));
   diff_cached_ = false;
 }
 
 void DmkTree::prepare_box_lists() {
   if (box_lists_ready_) return;
-  DevTree& D = dev_;
-  std::vector<int> c0(D.n_nodes);
-  PDMK_CUDA(cudaMemcpyAsync(c0.data(), D.node_child0, 4 * D.n_nodes, cudaMemcpyDeviceToHost, st_));
+  std::vector<int> c0(dev_.n_nodes);
+  PDMK_CUDA(cudaMemcpyAsync(c0.data(), dev_.node_child0, 4 * dev_.n_nodes, cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaStreamSynchronize(st_));
+  build_box_lists(c0);
+}
+
+void DmkTree::build_box_lists(const std::vector<int>& c0) {
+  DevTree& D = dev_;
   std::vector<int> nonleaf;
   if (D.pw_hi >= D.pw_lo)
     for (int id = D.level_start[D.pw_lo]; id < D.level_start[D.pw_hi + 1]; ++id)
@@ -933,8 +957,6 @@ void DmkTree::prepare_box_lists() {
   d_scalars_ = static_cast<double*>(alloc(sizeof(double) * 8));
   k_sum_q2<<<1, 1024, 0, st_>>>(D.sq, D.n_slots, d_scalars_ + 4);
   PDMK_LAUNCH_CHECK();
-  PDMK_CUDA(cudaMemcpyAsync(&Q_, d_scalars_ + 4, sizeof(double), cudaMemcpyDeviceToHost, st_));
-  PDMK_CUDA(cudaStreamSynchronize(st_));
   box_lists_ready_ = true;
 }
 
@@ -974,14 +996,17 @@ void DmkTree::form_incoming_pw() {
   diff_cached_ = true;
 }
 
-double DmkTree::eval_window_energy() {
+void DmkTree::launch_window_energy() {
   prepare_box_lists();
   DevTree& D = dev_;
   const double pi = 3.14159265358979323846;
   double scale = 1 / (2 * std::pow(2 * pi, 3)) * std::pow(D.delta_k[0], 3);
-  double self = Q_ * ps_.psi0_0 / (2 * D.boxsize[2] * ps_.C0);
-  k_window<<<1, 1024, 0, st_>>>(D, scale, self, d_scalars_ + 0);
+  k_window<<<1, 1024, 0, st_>>>(D, scale, d_scalars_ + 4, ps_.psi0_0, 2 * D.boxsize[2] * ps_.C0, d_scalars_ + 0);
   PDMK_LAUNCH_CHECK();
+}
+
+double DmkTree::eval_window_energy() {
+  launch_window_energy();
   double e;
   PDMK_CUDA(cudaMemcpyAsync(&e, d_scalars_ + 0, sizeof(double), cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaStreamSynchronize(st_));
@@ -997,8 +1022,7 @@ double DmkTree::eval_diff_energy() {
   return e;
 }
 
-double DmkTree::eval_res_energy() {
-  ensure_packed();
+void DmkTree::launch_res_energy() {
   prepare_box_lists();
   DevTree& D = dev_;
   if (n_leaves_ > 0) {
@@ -1009,7 +1033,14 @@ double DmkTree::eval_res_energy() {
     PDMK_LAUNCH_CHECK();
     k_sum<<<1, 1024, 0, st_>>>(D.partials, n_leaves_ * ny, d_scalars_ + 2);
     PDMK_LAUNCH_CHECK();
+  } else {
+    PDMK_CUDA(cudaMemsetAsync(d_scalars_ + 2, 0, sizeof(double), st_));
   }
+}
+
+double DmkTree::eval_res_energy() {
+  ensure_packed();
+  launch_res_energy();
   double e = 0;
   PDMK_CUDA(cudaMemcpyAsync(&e, d_scalars_ + 2, sizeof(double), cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaStreamSynchronize(st_));
@@ -1018,12 +1049,19 @@ double DmkTree::eval_res_energy() {
 
 EnergyParts DmkTree::eval_energy() {
   // per-box charge sums and the near field read particles from the slot
-  // ranges: fold any overflow-pool arrivals back into them first
+  // ranges: fold any overflow-pool arrivals back into them first. The three
+  // parts are enqueued back to back and read with one synchronisation.
   ensure_packed();
+  launch_window_energy();
+  if (!diff_cached_) run_incoming(false);
+  launch_res_energy();
+  double e[3];
+  PDMK_CUDA(cudaMemcpyAsync(e, d_scalars_, sizeof(e), cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
   EnergyParts p;
-  p.window = eval_window_energy();
-  p.diff = eval_diff_energy();
-  p.res = eval_res_energy();
+  p.window = e[0];
+  p.diff = e[1];
+  p.res = e[2];
   return p;
 }
 

@@ -1884,6 +1884,7 @@ void DmkTree::update_shift(long i, double dx, double dy, double dz) {
   PDMK_CUDA(cudaStreamSynchronize(st_));
   last_valid_ = false;
   diff_cached_ = false;
+  moved_ = true;
 }
 
 // One cooperative launch per kMcChunk moves on every SM (k_mc). The grid is
@@ -1945,6 +1946,7 @@ void DmkTree::mc_run_device(int n_moves, const int* d_idx, const double* d_disp,
     if (n_moves > 0) mc_run_persistent(n_moves, d_idx, d_disp, d_u, beta, d_dE, d_acc);
     last_valid_ = false;
     diff_cached_ = false;
+    moved_ = true;
     return;
   }
   ensure_move_resources();
@@ -1977,6 +1979,7 @@ void DmkTree::mc_run_device(int n_moves, const int* d_idx, const double* d_disp,
   }
   last_valid_ = false;
   diff_cached_ = false;
+  moved_ = true;
 }
 
 // All candidates in one launch of k_shift_batch (one block per candidate).
@@ -2139,6 +2142,7 @@ void DmkTree::replicas_mc_run(const std::vector<DmkTree*>& ts, int m, const int*
   for (DmkTree* t : ts) {
     t->last_valid_ = false;
     t->diff_cached_ = false;
+    t->moved_ = true;
   }
 }
 

@@ -252,6 +252,9 @@ class DmkTree {
   void launch_update();  // accept-and-update and membership commit, one launch
   void ensure_packed();
   void prepare_box_lists();
+  void build_box_lists(const std::vector<int>& child0);  // from a host copy of node_child0
+  void launch_window_energy();  // enqueue the window energy into d_scalars_[0]
+  void launch_res_energy();     // enqueue the near-field energy into d_scalars_[2]
   void run_incoming(bool write_inc);
 
   double L_;
@@ -282,6 +285,7 @@ class DmkTree {
   size_t partials_cap_ = 0;
   // energy bookkeeping
   bool diff_cached_ = false;
+  bool moved_ = false;  // moves ran since the last pack: the overflow pool may hold particles
   bool box_lists_ready_ = false;
   int n_nonleaf_ = 0, n_leaves_ = 0;
   int* d_nonleaf_ = nullptr;  // non-leaf nodes of the expansion levels
@@ -291,7 +295,6 @@ class DmkTree {
   double* d_Cl_ = nullptr;
   double* d_Sl_ = nullptr;
   double* d_scalars_ = nullptr;
-  double Q_ = 0;
   // optional CUDA-event timing per kernel class (0 shift, 1 update pair, 2 commit, 3 NUDFT)
  public:
   void set_timing(bool on) { timing_ = on; }
