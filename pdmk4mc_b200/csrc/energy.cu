@@ -693,12 +693,14 @@ __global__ void k_sum(const double* part, int n, double* out) {
   if (threadIdx.x == 0) *out = s;
 }
 
+// sum of q^2 over the slots: block b sums a grid-strided share into out[b]
+// (one block gives the total in out[0])
 __global__ void k_sum_q2(const double* sq, int n, double* out) {
   __shared__ double sm[32];
   double e = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) e += sq[i] * sq[i];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) e += sq[i] * sq[i];
   double s = block_sum(e, sm);
-  if (threadIdx.x == 0) *out = s;
+  if (threadIdx.x == 0) out[blockIdx.x] = s;
 }
 
 }  // namespace
@@ -955,7 +957,10 @@ void DmkTree::build_box_lists(const std::vector<int>& c0) {
   PDMK_CUDA(cudaMemcpyAsync(d_Cl_, Cl.data(), sizeof(double) * (MAX_LEVELS + 2), cudaMemcpyHostToDevice, st_));
   PDMK_CUDA(cudaMemcpyAsync(d_Sl_, Sl.data(), sizeof(double) * (MAX_LEVELS + 2), cudaMemcpyHostToDevice, st_));
   d_scalars_ = static_cast<double*>(alloc(sizeof(double) * 8));
-  k_sum_q2<<<1, 1024, 0, st_>>>(D.sq, D.n_slots, d_scalars_ + 4);
+  // sum(q^2) for the window self term: 64 block partials, then a fixed-order sum
+  k_sum_q2<<<64, 256, 0, st_>>>(D.sq, D.n_slots, D.partials);
+  PDMK_LAUNCH_CHECK();
+  k_sum<<<1, 1024, 0, st_>>>(D.partials, 64, d_scalars_ + 4);
   PDMK_LAUNCH_CHECK();
   box_lists_ready_ = true;
 }

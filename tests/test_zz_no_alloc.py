@@ -7,18 +7,18 @@ parity tests, and the single-move call (hpdmk_eval_shift_energy, the same
 kernel with the same fixed-order reductions) exactly; on consecutive calls
 and across trees that share the one static buffer. Kept in a file that sorts
 last so it also runs after every other GPU test."""
-
-ABS_DE = 2e-10  # energy shifts, absolute (as in the parity tests)
-
-
-def close(got, want, msg=""):
-    np.testing.assert_array_less(np.abs(got - want), ABS_DE * np.maximum(1.0, np.abs(want)), err_msg=msg)
 import numpy as np
 import pytest
 
 import pdmk4mc_b200 as P
 
 pytestmark = pytest.mark.gpu
+
+ABS_DE = 2e-10  # energy shifts, absolute (as in the parity tests)
+
+
+def close(got, want, msg=""):
+    np.testing.assert_array_less(np.abs(got - want), ABS_DE * np.maximum(1.0, np.abs(want)), err_msg=msg)
 
 
 def make_tree(n, L, npl, digits, seed):
