@@ -50,6 +50,7 @@ struct NudftWork {
   int row_tile;
   int pad_;
   double2* out;       // H complex outputs of this box (or of this split-K chunk)
+  const double2* tab; // factor tables of this item's particle chunks (shared by its row tiles)
 };
 
 // Each thread owns one (kz, ky) row and TC <= 20 of its kx columns: 4 TC FP64
@@ -104,10 +105,77 @@ __device__ inline void axis_factors(double xr, double dk, int M, int X, int m0, 
   }
 }
 
+// Factor tables of one particle chunk of a work item, in shared memory:
+// ex [KC][DP], ey [KC][DP], ez [KC][NK+1] (charge folded into ez), rows past
+// the item's last particle and the padding columns D .. DP-1 zero. Tasks are
+// (particle, axis, half) so that each recurrence chain covers half an axis.
 template <int NK>
-__global__ void __launch_bounds__(NudftShape<NK>::THREADS)
-    k_nudft(const NudftWork* __restrict__ work, const double* __restrict__ sx, const double* __restrict__ sy,
-            const double* __restrict__ sz, const double* __restrict__ sq) {
+__device__ void nudft_build(const NudftWork& w, int base, double2* buf, const double* __restrict__ sx,
+                            const double* __restrict__ sy, const double* __restrict__ sz,
+                            const double* __restrict__ sq) {
+  using S = NudftShape<NK>;
+  double2* ex = buf;
+  double2* ey = ex + S::KC * S::DP;
+  double2* ez = ey + S::KC * S::DP;
+  const int nk = min(S::KC, w.s_end - base);
+  for (int t = threadIdx.x; t < S::KC * 6; t += blockDim.x) {
+    int j = t / 6, a = (t / 2) % 3, half = t & 1;
+    if (j >= nk) {
+      double2* dst = a == 0 ? ex + j * S::DP : (a == 1 ? ey + j * S::DP : ez + j * (NK + 1));
+      int len = a == 2 ? NK + 1 : S::DP;
+      for (int u = half; u < len; u += 2) dst[u] = make_double2(0.0, 0.0);
+      continue;
+    }
+    int s = base + j;
+    if (a == 0) {
+      int h = (S::D + 1) / 2;
+      int m0 = half ? -NK + h : -NK, cnt = half ? S::D - h : h;
+      axis_factors(sx[s] - w.cx, w.dk, w.M, w.X, m0, cnt, 1.0, ex + j * S::DP + (m0 + NK));
+      if (half)
+        for (int u = S::D; u < S::DP; ++u) ex[j * S::DP + u] = make_double2(0.0, 0.0);
+    } else if (a == 1) {
+      int h = (S::D + 1) / 2;
+      int m0 = half ? -NK + h : -NK, cnt = half ? S::D - h : h;
+      axis_factors(sy[s] - w.cy, w.dk, w.M, w.Y, m0, cnt, 1.0, ey + j * S::DP + (m0 + NK));
+    } else {
+      int h = (NK + 2) / 2;
+      int m0 = half ? -NK + h : -NK, cnt = half ? NK + 1 - h : h;
+      axis_factors(sz[s] - w.cz, w.dk, w.M, w.Z, m0, cnt, sq[s], ez + j * (NK + 1) + (m0 + NK));
+    }
+  }
+}
+
+// Table pass: one block per (item, particle chunk) builds the chunk's tables
+// in shared memory and writes them to the item's table range in HBM with
+// coalesced stores, once for all row tiles of the item.
+template <int NK>
+__global__ void __launch_bounds__(NudftShape<NK>::KC * 6)
+    k_nudft_tables(const NudftWork* __restrict__ work, const int2* __restrict__ chunks, const double* __restrict__ sx,
+                   const double* __restrict__ sy, const double* __restrict__ sz, const double* __restrict__ sq) {
+  using S = NudftShape<NK>;
+  constexpr int BUF = S::KC * (2 * S::DP + NK + 1);
+  extern __shared__ double2 smem[];
+  const int2 ch = chunks[blockIdx.x];
+  const NudftWork w = work[ch.x];
+  nudft_build<NK>(w, w.s_begin + ch.y * S::KC, smem, sx, sy, sz, sq);
+  __syncthreads();
+  double2* dst = const_cast<double2*>(w.tab) + size_t(ch.y) * BUF;
+  for (int i = threadIdx.x; i < BUF; i += blockDim.x) dst[i] = smem[i];
+}
+
+__device__ inline void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  const size_t g = __cvta_generic_to_global(gmem_src);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(g) : "memory");
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ inline void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Contraction pass: one (item, row tile) per block. The chunk tables stream
+// from HBM into two shared-memory buffers by asynchronous copies issued a
+// chunk ahead, so every thread does the same work between two barriers.
+template <int NK>
+__global__ void __launch_bounds__(NudftShape<NK>::THREADS) k_nudft(const NudftWork* __restrict__ work) {
   using S = NudftShape<NK>;
   constexpr int BUF = S::KC * (2 * S::DP + NK + 1);  // complex entries per table buffer
   extern __shared__ double2 smem[];
@@ -118,52 +186,28 @@ __global__ void __launch_bounds__(NudftShape<NK>::THREADS)
   const int cg = active ? g % S::CG : 0;
   const int kz = row / S::D, ky = row % S::D;
   const int c0 = cg * S::TC;
-  // factor tables of one particle chunk: ex [KC][DP], ey [KC][DP], ez [KC][NK+1]
-  // (charge folded into ez); two buffers so the next chunk's tables are
-  // built while the current chunk is contracted (one barrier per chunk)
-  auto build = [&](int base, double2* buf) {
-    double2* ex = buf;
-    double2* ey = ex + S::KC * S::DP;
-    double2* ez = ey + S::KC * S::DP;
-    const int nk = min(S::KC, w.s_end - base);
-    for (int t = threadIdx.x; t < S::KC * 6; t += blockDim.x) {
-      int j = t / 6, a = (t / 2) % 3, half = t & 1;
-      if (j >= nk) {
-        double2* dst = a == 0 ? ex + j * S::DP : (a == 1 ? ey + j * S::DP : ez + j * (NK + 1));
-        int len = a == 2 ? NK + 1 : S::DP;
-        for (int u = half; u < len; u += 2) dst[u] = make_double2(0.0, 0.0);
-        continue;
-      }
-      int s = base + j;
-      if (a == 0) {
-        int h = (S::D + 1) / 2;
-        int m0 = half ? -NK + h : -NK, cnt = half ? S::D - h : h;
-        axis_factors(sx[s] - w.cx, w.dk, w.M, w.X, m0, cnt, 1.0, ex + j * S::DP + (m0 + NK));
-        if (half)
-          for (int u = S::D; u < S::DP; ++u) ex[j * S::DP + u] = make_double2(0.0, 0.0);
-      } else if (a == 1) {
-        int h = (S::D + 1) / 2;
-        int m0 = half ? -NK + h : -NK, cnt = half ? S::D - h : h;
-        axis_factors(sy[s] - w.cy, w.dk, w.M, w.Y, m0, cnt, 1.0, ey + j * S::DP + (m0 + NK));
-      } else {
-        int h = (NK + 2) / 2;
-        int m0 = half ? -NK + h : -NK, cnt = half ? NK + 1 - h : h;
-        axis_factors(sz[s] - w.cz, w.dk, w.M, w.Z, m0, cnt, sq[s], ez + j * (NK + 1) + (m0 + NK));
-      }
-    }
+  const int nch = (w.s_end - w.s_begin + S::KC - 1) / S::KC;
+  auto fetch = [&](int c) {
+    const double2* src = w.tab + size_t(c) * BUF;
+    double2* dst = smem + (c & 1) * BUF;
+    for (int i = threadIdx.x; i < BUF; i += blockDim.x) cp_async16(dst + i, src + i);
   };
   double2 acc[S::TC];
 #pragma unroll
   for (int c = 0; c < S::TC; ++c) acc[c] = make_double2(0.0, 0.0);
-  if (w.s_begin < w.s_end) build(w.s_begin, smem);
-  __syncthreads();
-  int cur = 0;
-  for (int base = w.s_begin; base < w.s_end; base += S::KC) {
-    if (base + S::KC < w.s_end) build(base + S::KC, smem + (cur ^ 1) * BUF);
-    const double2* ex = smem + cur * BUF;
+  if (nch > 0) fetch(0);
+  cp_async_commit();
+  for (int ci = 0; ci < nch; ++ci) {
+    // the next chunk's copies go out before this chunk is contracted (its
+    // buffer was last read before the previous iteration's closing barrier)
+    if (ci + 1 < nch) fetch(ci + 1);
+    cp_async_commit();
+    cp_async_wait_prior();  // everything but the group just committed has landed
+    __syncthreads();
+    const double2* ex = smem + (ci & 1) * BUF;
     const double2* ey = ex + S::KC * S::DP;
     const double2* ez = ey + S::KC * S::DP;
-    const int nk = min(S::KC, w.s_end - base);
+    const int nk = min(S::KC, w.s_end - (w.s_begin + ci * S::KC));
     if (active) {
 #pragma unroll 1
       for (int j = 0; j < nk; ++j) {
@@ -182,7 +226,6 @@ __global__ void __launch_bounds__(NudftShape<NK>::THREADS)
       }
     }
     __syncthreads();
-    cur ^= 1;
   }
   if (active) {
     double2* o = w.out + size_t(row) * S::D + c0;
@@ -193,46 +236,92 @@ __global__ void __launch_bounds__(NudftShape<NK>::THREADS)
 }
 
 template <int NK>
-void launch_nudft(const NudftWork* d_work, int nwork, const DevTree& T, cudaStream_t st) {
+void launch_nudft(const NudftWork* d_work, int nwork, const int2* d_chunks, int nchunks, const DevTree& T,
+                  cudaStream_t st) {
   using S = NudftShape<NK>;
+  constexpr int TAB_SMEM = S::KC * (2 * S::DP + NK + 1) * int(sizeof(double2));
   if (nwork == 0) return;
   static bool attr = false;
   if (!attr) {
     PDMK_CUDA(cudaFuncSetAttribute(k_nudft<NK>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
+    PDMK_CUDA(cudaFuncSetAttribute(k_nudft_tables<NK>, cudaFuncAttributeMaxDynamicSharedMemorySize, TAB_SMEM));
     attr = true;
   }
-  k_nudft<NK><<<unsigned(nwork), S::THREADS, S::SMEM, st>>>(d_work, T.sx, T.sy, T.sz, T.sq);
+  if (nchunks > 0) {
+    k_nudft_tables<NK><<<unsigned(nchunks), S::KC * 6, TAB_SMEM, st>>>(d_work, d_chunks, T.sx, T.sy, T.sz, T.sq);
+    PDMK_LAUNCH_CHECK();
+  }
+  k_nudft<NK><<<unsigned(nwork), S::THREADS, S::SMEM, st>>>(d_work);
   PDMK_LAUNCH_CHECK();
 }
 
-void dispatch_nudft(int nk, const NudftWork* d_work, int nwork, const DevTree& T, cudaStream_t st) {
+struct NudftInfo {
+  int tiles, kc, buf;  // row tiles per item, particles per chunk, complex entries per chunk table
+};
+
+template <int NK>
+NudftInfo nudft_info_of() {
+  using S = NudftShape<NK>;
+  return {S::TILES, S::KC, S::KC * (2 * S::DP + NK + 1)};
+}
+
+NudftInfo nudft_info(int nk) {
   switch (nk) {
-    case 4: launch_nudft<4>(d_work, nwork, T, st); break;
-    case 6: launch_nudft<6>(d_work, nwork, T, st); break;
-    case 8: launch_nudft<8>(d_work, nwork, T, st); break;
-    case 12: launch_nudft<12>(d_work, nwork, T, st); break;
-    case 13: launch_nudft<13>(d_work, nwork, T, st); break;
-    case 17: launch_nudft<17>(d_work, nwork, T, st); break;
-    case 19: launch_nudft<19>(d_work, nwork, T, st); break;
-    case 26: launch_nudft<26>(d_work, nwork, T, st); break;
-    case 32: launch_nudft<32>(d_work, nwork, T, st); break;  // Ewald structure factor, level 2
-    case 64: launch_nudft<64>(d_work, nwork, T, st); break;  // Ewald structure factor, level 3
+    case 4: return nudft_info_of<4>();
+    case 6: return nudft_info_of<6>();
+    case 8: return nudft_info_of<8>();
+    case 12: return nudft_info_of<12>();
+    case 13: return nudft_info_of<13>();
+    case 17: return nudft_info_of<17>();
+    case 19: return nudft_info_of<19>();
+    case 26: return nudft_info_of<26>();
+    case 32: return nudft_info_of<32>();  // Ewald structure factor, level 2
+    case 64: return nudft_info_of<64>();  // Ewald structure factor, level 3
     default: throw std::invalid_argument("unsupported mode count");
   }
 }
 
-int nudft_tiles(int nk) {
+int nudft_tiles(int nk) { return nudft_info(nk).tiles; }
+
+// Lays out the factor tables of a work list whose items are runs of `tiles`
+// consecutive entries (row tiles 0 .. tiles-1 of one box or chunk): each item
+// gets ceil(n / KC) chunk tables, allocated here stream-ordered on `st`, and
+// the list of (first entry, chunk) pairs the table pass runs over. The caller
+// frees `tables` stream-ordered after the contraction.
+void plan_nudft_tables(int nk, std::vector<NudftWork>& wl, double2** tables, std::vector<int2>& chunks,
+                       cudaStream_t st) {
+  const NudftInfo in = nudft_info(nk);
+  size_t nchunk = 0;
+  for (size_t e = 0; e < wl.size(); e += in.tiles) {
+    if (wl[e].row_tile != 0) throw std::logic_error("NUDFT work list: items must start at row tile 0");
+    nchunk += size_t((wl[e].s_end - wl[e].s_begin + in.kc - 1) / in.kc);
+  }
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(tables), sizeof(double2) * size_t(in.buf) * std::max<size_t>(nchunk, 1),
+                            st));
+  chunks.clear();
+  chunks.reserve(nchunk);
+  size_t c = 0;
+  for (size_t e = 0; e < wl.size(); e += in.tiles) {
+    const int n = (wl[e].s_end - wl[e].s_begin + in.kc - 1) / in.kc;
+    for (int t = 0; t < in.tiles && e + t < wl.size(); ++t) wl[e + t].tab = *tables + c * size_t(in.buf);
+    for (int k = 0; k < n; ++k) chunks.push_back(make_int2(int(e), k));
+    c += size_t(n);
+  }
+}
+
+void dispatch_nudft(int nk, const NudftWork* d_work, int nwork, const int2* d_chunks, int nchunks, const DevTree& T,
+                    cudaStream_t st) {
   switch (nk) {
-    case 4: return NudftShape<4>::TILES;
-    case 6: return NudftShape<6>::TILES;
-    case 8: return NudftShape<8>::TILES;
-    case 12: return NudftShape<12>::TILES;
-    case 13: return NudftShape<13>::TILES;
-    case 17: return NudftShape<17>::TILES;
-    case 19: return NudftShape<19>::TILES;
-    case 26: return NudftShape<26>::TILES;
-    case 32: return NudftShape<32>::TILES;
-    case 64: return NudftShape<64>::TILES;
+    case 4: launch_nudft<4>(d_work, nwork, d_chunks, nchunks, T, st); break;
+    case 6: launch_nudft<6>(d_work, nwork, d_chunks, nchunks, T, st); break;
+    case 8: launch_nudft<8>(d_work, nwork, d_chunks, nchunks, T, st); break;
+    case 12: launch_nudft<12>(d_work, nwork, d_chunks, nchunks, T, st); break;
+    case 13: launch_nudft<13>(d_work, nwork, d_chunks, nchunks, T, st); break;
+    case 17: launch_nudft<17>(d_work, nwork, d_chunks, nchunks, T, st); break;
+    case 19: launch_nudft<19>(d_work, nwork, d_chunks, nchunks, T, st); break;
+    case 26: launch_nudft<26>(d_work, nwork, d_chunks, nchunks, T, st); break;
+    case 32: launch_nudft<32>(d_work, nwork, d_chunks, nchunks, T, st); break;
+    case 64: launch_nudft<64>(d_work, nwork, d_chunks, nchunks, T, st); break;
     default: throw std::invalid_argument("unsupported mode count");
   }
 }
@@ -852,11 +941,20 @@ void DmkTree::form_outgoing_pw() {
       }
     }
   }
-  // one upload: the work items (boxes first, then the root chunks), then per
-  // split-K group its first chunk, chunk count and output, for the reductions
+  // factor tables of both passes (allocated here on st_, so the root pass on
+  // the second stream is ordered after the allocation by the fork event)
+  double2 *tab_box = nullptr, *tab_root = nullptr;
+  std::vector<int2> ch_box, ch_root;
+  plan_nudft_tables(D.n_diff, wbox, &tab_box, ch_box, st_);
+  plan_nudft_tables(D.n_window, wroot, &tab_root, ch_root, st_);
+  // one upload: the work items (boxes first, then the root chunks), their
+  // table chunk lists, then per split-K group its first chunk, chunk count
+  // and output, for the reductions
   const size_t nw = wroot.size() + wbox.size();
   auto align16 = [](size_t b) { return (b + 15) & ~size_t(15); };
-  const size_t off_rmeta = align16(sizeof(NudftWork) * nw);
+  const size_t off_cbox = align16(sizeof(NudftWork) * nw);
+  const size_t off_croot = align16(off_cbox + sizeof(int2) * ch_box.size());
+  const size_t off_rmeta = align16(off_croot + sizeof(int2) * ch_root.size());
   const size_t off_rout = align16(off_rmeta + sizeof(int) * 2 * root_split.size());
   const size_t off_bmeta = align16(off_rout + sizeof(double2*) * root_split.size());
   const size_t off_bout = align16(off_bmeta + sizeof(int) * 2 * box_split.size());
@@ -864,6 +962,8 @@ void DmkTree::form_outgoing_pw() {
   std::vector<unsigned char> blob(blob_bytes, 0);
   std::memcpy(blob.data(), wbox.data(), sizeof(NudftWork) * wbox.size());
   std::memcpy(blob.data() + sizeof(NudftWork) * wbox.size(), wroot.data(), sizeof(NudftWork) * wroot.size());
+  std::memcpy(blob.data() + off_cbox, ch_box.data(), sizeof(int2) * ch_box.size());
+  std::memcpy(blob.data() + off_croot, ch_root.data(), sizeof(int2) * ch_root.size());
   auto put_meta = [&](const std::vector<Chunked>& sp, size_t off_meta, size_t off_out) {
     int* meta = reinterpret_cast<int*>(blob.data() + off_meta);
     double2** outs = reinterpret_cast<double2**>(blob.data() + off_out);
@@ -887,10 +987,12 @@ void DmkTree::form_outgoing_pw() {
   }
   PDMK_CUDA(cudaEventRecord(ev_fork_, st_));
   PDMK_CUDA(cudaStreamWaitEvent(aux_, ev_fork_, 0));
-  dispatch_nudft(D.n_window, d_work + wbox.size(), int(wroot.size()), D, aux_);
+  dispatch_nudft(D.n_window, d_work + wbox.size(), int(wroot.size()), reinterpret_cast<const int2*>(d_blob + off_croot),
+                 int(ch_root.size()), D, aux_);
   PDMK_CUDA(cudaEventRecord(ev_join_, aux_));
   time_begin(3);
-  dispatch_nudft(D.n_diff, d_work, int(wbox.size()), D, st_);
+  dispatch_nudft(D.n_diff, d_work, int(wbox.size()), reinterpret_cast<const int2*>(d_blob + off_cbox),
+                 int(ch_box.size()), D, st_);
   time_end(3);
   PDMK_CUDA(cudaStreamWaitEvent(st_, ev_join_, 0));
   // reduce split-K chunks
@@ -906,6 +1008,8 @@ void DmkTree::form_outgoing_pw() {
   reduce(root_split, part, D.Hw, off_rmeta, off_rout);
   reduce(box_split, part_b, D.H, off_bmeta, off_bout);
   PDMK_CUDA(cudaFreeAsync(d_blob, st_));
+  PDMK_CUDA(cudaFreeAsync(tab_box, st_));
+  PDMK_CUDA(cudaFreeAsync(tab_root, st_));
   PDMK_CUDA(cudaFreeAsync(part, st_));
   diff_cached_ = false;
 }
@@ -1116,11 +1220,21 @@ double DmkTree::ewald_energy(double* parts) {
   double* sums = nullptr;
   PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double2) * size_t(Hs) * nch, st_));
   PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&S), sizeof(double2) * size_t(Hs), st_));
-  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_work), sizeof(NudftWork) * wl.size(), st_));
   PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&sums), sizeof(double) * (nblk_real + nblk_rec + 8), st_));
   for (size_t i = 0; i < wl.size(); ++i) wl[i].out = part + size_t(i / tiles) * Hs;
-  PDMK_CUDA(cudaMemcpyAsync(d_work, wl.data(), sizeof(NudftWork) * wl.size(), cudaMemcpyHostToDevice, st_));
-  dispatch_nudft(nk, d_work, int(wl.size()), D, st_);
+  double2* tab = nullptr;
+  std::vector<int2> chunks;
+  plan_nudft_tables(nk, wl, &tab, chunks, st_);
+  const size_t off_ch = (sizeof(NudftWork) * wl.size() + 15) & ~size_t(15);
+  std::vector<unsigned char> blob(off_ch + sizeof(int2) * chunks.size() + 16, 0);
+  std::memcpy(blob.data(), wl.data(), sizeof(NudftWork) * wl.size());
+  std::memcpy(blob.data() + off_ch, chunks.data(), sizeof(int2) * chunks.size());
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_work), blob.size(), st_));
+  PDMK_CUDA(cudaMemcpyAsync(d_work, blob.data(), blob.size(), cudaMemcpyHostToDevice, st_));
+  dispatch_nudft(nk, d_work, int(wl.size()),
+                 reinterpret_cast<const int2*>(reinterpret_cast<unsigned char*>(d_work) + off_ch), int(chunks.size()),
+                 D, st_);
+  PDMK_CUDA(cudaFreeAsync(tab, st_));
   {
     int* d_meta;
     double2** d_outs;
