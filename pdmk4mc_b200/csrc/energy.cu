@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
   __shared__ double ux[RES_SCH], uy[RES_SCH], uz[RES_SCH], uq[RES_SCH];
   __shared__ int uslot[RES_SCH];
   __shared__ int m_beg[36], m_pre[37];
-  __shared__ double m_off[36][3];
+  __shared__ double m_off[36][3], m_w[36];
   __shared__ double sm[32];
   const ResidualPoly<NP> poly(T);
   const int node = leaves[blockIdx.x / ny], chunk = blockIdx.x % ny;
@@ -558,9 +558,16 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
       if (src == 0) j = node;
       else if (src <= 27) j = (src - 1 == 13) ? -1 : T.col27[size_t(node) * 27 + (src - 1)];
       else j = T.coarse8[size_t(node) * 8 + (src - 28)];
+      // A pair of particles in two leaves of the same level meets the same
+      // cut-off from either side, so only the leaf with the smaller id sums
+      // it, with weight 2. Other sources (non-leaf colleagues, coarser
+      // neighbours) see a cut-off that depends on the target's level: both
+      // sides sum those.
+      const bool same_level_leaf = src >= 1 && src <= 27 && j >= 0 && T.node_child0[j] < 0;
+      const bool skip = same_level_leaf && j < node;
       int beg = 0, n = 0;
       double off[3] = {0, 0, 0};
-      if (j >= 0 && T.node_count[j] > 0) {
+      if (j >= 0 && !skip && T.node_count[j] > 0) {
         double ci[3], cj[3];
         node_center(T, node, ci);
         node_center(T, j, cj);
@@ -571,6 +578,7 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
       }
       m_beg[src] = beg;
       m_pre[src] = n;
+      m_w[src] = same_level_leaf ? 2.0 : 1.0;
       for (int dd = 0; dd < 3; ++dd) m_off[src][dd] = off[dd];
     }
     __syncthreads();
@@ -616,7 +624,7 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
           ux[t] = T.sx[s] + m_off[lo][0];
           uy[t] = T.sy[s] + m_off[lo][1];
           uz[t] = T.sz[s] + m_off[lo][2];
-          uq[t] = T.sq[s];
+          uq[t] = T.sq[s] * m_w[lo];
           uslot[t] = lo == 0 ? s : -1;
         }
         __syncthreads();
