@@ -106,10 +106,14 @@ __device__ inline int cell_rank(const Bitmaps& B, int level, uint64_t cell) {
 }
 
 // candidates at `level` are the 8 children of each refined cell of the level above
+// The parent count comes from the device (the previous level's out_n), so
+// levels can be launched back to back; lists hold at most list_cap cells and
+// the host checks the counts for overflow when it reads them.
 __global__ void k_refine_level(const uint64_t* keys, long n, int level, int n_per_leaf, const uint64_t* parents,
-                               int n_parents, uint32_t* bm, uint64_t* out_list, int* out_n) {
+                               const int* n_parents, int list_cap, uint32_t* bm, uint64_t* out_list, int* out_n) {
   long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= long(n_parents) * 8) return;
+  const int np = min(*n_parents, list_cap);
+  if (t >= long(np) * 8) return;
   uint64_t cell = (parents[t >> 3] << 3) | uint64_t(t & 7);
   long lo, hi;
   cell_range(keys, n, level, cell, &lo, &hi);
@@ -117,7 +121,7 @@ __global__ void k_refine_level(const uint64_t* keys, long n, int level, int n_pe
   if (refine) {
     bit_set(bm, cell);
     int k = atomicAdd(out_n, 1);
-    out_list[k] = cell;
+    if (k < list_cap) out_list[k] = cell;
   }
 }
 
@@ -546,31 +550,47 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
   put_small(lists[0], &zero, 8, st_);
   int maxref = 0;  // deepest level holding a refined cell
   {
+    // refined cells per level (level 0: the root), on the device
+    int* d_lvl;
+    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_lvl), sizeof(int) * (MAX_LEVEL + 2), st_));
+    PDMK_CUDA(cudaMemsetAsync(d_lvl, 0, sizeof(int) * (MAX_LEVEL + 2), st_));
+    const int one = 1;
+    put_small(d_lvl, &one, 4, st_);
     // root: refined (all nodes above level 2 are refined)
     B.bm[0] = static_cast<uint32_t*>(alloc(4));
-    uint32_t one = 1;
     put_small(B.bm[0], &one, 4, st_);
-    int n_par = 1;
-    int cur = 0;
-    for (int l = 1; l <= MAX_LEVEL; ++l) {
-      long ncand = long(n_par) * 8;
-      if (ncand > list_cap) throw std::runtime_error("tree build: refinement list overflow");
+    auto refine = [&](int l, unsigned grid) {
       if (l < MAX_LEVEL) {
         B.bm[l] = static_cast<uint32_t*>(alloc(size_t(nwords[l]) * 4));
         PDMK_CUDA(cudaMemsetAsync(B.bm[l], 0, size_t(nwords[l]) * 4, st_));
       }
-      PDMK_CUDA(cudaMemsetAsync(d_cnt, 0, 4, st_));
-      k_refine_level<<<grid_for(ncand), TPB, 0, st_>>>(keys, n, l, n_per_leaf_, lists[cur], n_par,
-                                                       l < MAX_LEVEL ? B.bm[l] : nullptr, lists[cur ^ 1], d_cnt);
+      k_refine_level<<<grid, TPB, 0, st_>>>(keys, n, l, n_per_leaf_, lists[(l - 1) & 1], d_lvl + (l - 1), int(list_cap),
+                                             l < MAX_LEVEL ? B.bm[l] : nullptr, lists[l & 1], d_lvl + l);
       PDMK_LAUNCH_CHECK();
-      int h_cnt = 0;
-      PDMK_CUDA(cudaMemcpyAsync(&h_cnt, d_cnt, 4, cudaMemcpyDeviceToHost, st_));
-      PDMK_CUDA(cudaStreamSynchronize(st_));
-      if (h_cnt == 0) break;
+    };
+    // the shallow levels (bitmaps of at most 32 KB) go back to back with one
+    // read-back; deeper trees continue level by level
+    constexpr int kEager = 6;
+    for (int l = 1; l <= kEager; ++l) refine(l, grid_for(list_cap));
+    int cnt[MAX_LEVEL + 2] = {0};
+    PDMK_CUDA(cudaMemcpyAsync(cnt, d_lvl, sizeof(int) * (kEager + 1), cudaMemcpyDeviceToHost, st_));
+    PDMK_CUDA(cudaStreamSynchronize(st_));
+    for (int l = 1; l <= kEager; ++l) {
+      if (long(cnt[l - 1]) * 8 > list_cap || cnt[l] > list_cap)
+        throw std::runtime_error("tree build: refinement list overflow");
+      if (cnt[l] == 0) break;
       maxref = l;
-      n_par = h_cnt;
-      cur ^= 1;
     }
+    for (int l = kEager + 1; maxref == l - 1 && l <= MAX_LEVEL; ++l) {
+      const long ncand = long(cnt[l - 1]) * 8;
+      if (ncand > list_cap) throw std::runtime_error("tree build: refinement list overflow");
+      refine(l, grid_for(ncand));
+      PDMK_CUDA(cudaMemcpyAsync(cnt + l, d_lvl + l, 4, cudaMemcpyDeviceToHost, st_));
+      PDMK_CUDA(cudaStreamSynchronize(st_));
+      if (cnt[l] > list_cap) throw std::runtime_error("tree build: refinement list overflow");
+      if (cnt[l] > 0) maxref = l;
+    }
+    PDMK_CUDA(cudaFreeAsync(d_lvl, st_));
   }
   // 2:1 balance, deepest refined level first
   for (int k = maxref; k >= 2; --k) {

@@ -1,6 +1,7 @@
-// Exclusive scan (reduce-then-scan, three launches) and stable LSD radix
-// sort with 8-bit digits (tile histogram -> digit-major scan -> stable
-// warp-multisplit scatter). Used to bin particles by Morton key.
+// Exclusive scan (one launch up to 4096 items, else reduce-then-scan in three
+// launches) and stable LSD radix sort with 8-bit digits (tile histogram ->
+// digit-major scan -> stable warp-multisplit scatter). Used to bin particles
+// by Morton key.
 #include "common.cuh"
 #include "sort.cuh"
 
@@ -85,6 +86,25 @@ __global__ void k_scan_apply(const int* in, int* out, long n, const int* bsum) {
   }
 }
 
+// one tile (n <= SCAN_TILE): the whole scan in one block
+__global__ void k_scan_one(const int* in, int* out, int n) {
+  __shared__ int sm[32];
+  int v[SCAN_ITEMS];
+  int s = 0;
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    int i = threadIdx.x * SCAN_ITEMS + k;
+    v[k] = i < n ? in[i] : 0;
+    s += v[k];
+  }
+  __syncthreads();  // in and out may alias: all loads before any store
+  int off = block_exclusive_scan_1024(s, sm, nullptr);
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    int i = threadIdx.x * SCAN_ITEMS + k;
+    if (i < n) out[i] = off;
+    off += v[k];
+  }
+}
+
 // ---------------------------------------------------------------------------
 constexpr int RS_T = 256;       // threads per tile
 constexpr int RS_ITEMS = 8;     // items per thread
@@ -164,6 +184,11 @@ void exclusive_scan(const int* in, int* out, long n, void* scratch, cudaStream_t
   if (n <= 0) return;
   long nb = (n + SCAN_TILE - 1) / SCAN_TILE;
   if (nb > SCAN_TILE) throw std::invalid_argument("exclusive_scan: input too long");
+  if (nb == 1) {
+    k_scan_one<<<1, SCAN_T, 0, st>>>(in, out, int(n));
+    PDMK_LAUNCH_CHECK();
+    return;
+  }
   int* bsum = static_cast<int*>(scratch);
   k_block_sums<<<unsigned(nb), SCAN_T, 0, st>>>(in, n, bsum);
   PDMK_LAUNCH_CHECK();

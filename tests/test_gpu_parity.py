@@ -48,6 +48,26 @@ CASES = [
 ]
 
 
+def test_tree_bit_exact_deep():
+    # a tight cluster refines down to the deepest allowed level: the levels
+    # past the first read-back of the refinement counts, and the level cap
+    rng = np.random.default_rng(4)
+    L, n = 10.0, 3000
+    r = np.concatenate([np.mod(np.array([3.0, 6.0, 4.5]) + rng.normal(0, L / 3000, (2000, 3)), L),
+                        rng.uniform(0, L, (n - 2000, 3))]).reshape(-1)
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    g = P.HPDMKPtTree(P.HPDMKParams(n_per_leaf=10, digits=6, L=L, init=P.DIRECT), r, q)
+    o = O.OracleTree(L, 10, 6, r, q)
+    assert g.max_depth == o.max_depth and g.max_depth >= 10
+    assert g.n_nodes == o.n_nodes
+    for a, b in zip(g.tree_nodes(), o.tree_nodes()):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(g.tree_neighbors(), o.tree_neighbors()):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(g.sorted_order(), o.sorted_order())
+    g.close()
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_tree_bit_exact(case):
     g, o, r, q = pair(*case)
