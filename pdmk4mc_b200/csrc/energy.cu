@@ -840,43 +840,14 @@ void DmkTree::ensure_packed() {
 void DmkTree::form_outgoing_pw() {
   ensure_packed();
   DevTree& D = dev_;
-  // host view of node slot ranges and coordinates for the work list (and, on
-  // a new tree, of the children for the box lists: one round trip for both)
-  const int nn = D.n_nodes;
-  std::vector<int> nb(nn), ne(nn), lv(nn), c0;
-  std::vector<uint64_t> pf(nn);
-  PDMK_CUDA(cudaMemcpyAsync(nb.data(), D.node_begin, 4 * nn, cudaMemcpyDeviceToHost, st_));
-  PDMK_CUDA(cudaMemcpyAsync(ne.data(), D.node_end, 4 * nn, cudaMemcpyDeviceToHost, st_));
-  PDMK_CUDA(cudaMemcpyAsync(lv.data(), D.node_level, 4 * nn, cudaMemcpyDeviceToHost, st_));
-  PDMK_CUDA(cudaMemcpyAsync(pf.data(), D.node_prefix, 8 * nn, cudaMemcpyDeviceToHost, st_));
-  if (!box_lists_ready_) {
-    c0.resize(nn);
-    PDMK_CUDA(cudaMemcpyAsync(c0.data(), D.node_child0, 4 * nn, cudaMemcpyDeviceToHost, st_));
-  }
-  PDMK_CUDA(cudaStreamSynchronize(st_));
-  if (!box_lists_ready_) build_box_lists(c0);
-  struct Box {
-    int node, sb, se, level;
-    double2* out;
-  };
-  // root split into chunks + boxes of the expansion levels
-  std::vector<Box> boxes;
-  const int base = D.level_start[D.pw_lo];
-  if (D.pw_hi >= D.pw_lo)
-    for (int id = base; id < D.level_start[D.pw_hi + 1]; ++id)
-      boxes.push_back({id, nb[id], ne[id], lv[id], D.out + size_t(id - base) * D.H});
   // split-K bookkeeping: chunks go to a partial buffer, then reduce
   struct Chunked {
     int first, n;
     double2* out;
   };
-  std::vector<Chunked> root_split, box_split;
-  std::vector<NudftWork> wroot, wbox;
-  long part_root = 0, part_box = 0;
-  auto make_work = [&](std::vector<NudftWork>& wl, int nk, const Box& bx, double2* out, int sb, int se) {
+  // the row tiles of one box (or box chunk) over the slots [sb, se)
+  auto make_work = [&](std::vector<NudftWork>& wl, int nk, int l, uint64_t p, double2* out, int sb, int se) {
     NudftWork w{};
-    int l = bx.level;
-    uint64_t p = pf[bx.node];
     double scale = std::ldexp(1.0, -l);
     int X = int(compact3(p)), Y = int(compact3(p >> 1)), Z = int(compact3(p >> 2));
     w.cx = L_ * (double(X) * scale + 0.5 * scale);
@@ -896,17 +867,100 @@ void DmkTree::form_outgoing_pw() {
       wl.push_back(w);
     }
   };
-  // root over all slots
-  {
-    int nch = std::max(1, (D.n_slots + KSPLIT_ROOT - 1) / KSPLIT_ROOT);
-    root_split.push_back({0, nch, D.out_root});
-    part_root = long(nch) * D.Hw;
+  auto align16 = [](size_t b) { return (b + 15) & ~size_t(15); };
+  // one upload per pass: the work items, their table chunk lists, then per
+  // split-K group its first chunk, chunk count and output
+  auto upload = [&](const std::vector<NudftWork>& wl, const std::vector<int2>& ch, const std::vector<Chunked>& sp,
+                    size_t* off_ch, size_t* off_meta, size_t* off_out) {
+    *off_ch = align16(sizeof(NudftWork) * wl.size());
+    *off_meta = align16(*off_ch + sizeof(int2) * ch.size());
+    *off_out = align16(*off_meta + sizeof(int) * 2 * sp.size());
+    const size_t bytes = align16(*off_out + sizeof(double2*) * sp.size()) + 16;
+    std::vector<unsigned char> blob(bytes, 0);
+    std::memcpy(blob.data(), wl.data(), sizeof(NudftWork) * wl.size());
+    std::memcpy(blob.data() + *off_ch, ch.data(), sizeof(int2) * ch.size());
+    int* meta = reinterpret_cast<int*>(blob.data() + *off_meta);
+    double2** outs = reinterpret_cast<double2**>(blob.data() + *off_out);
+    for (size_t i = 0; i < sp.size(); ++i) {
+      meta[i] = sp[i].first;
+      meta[sp.size() + i] = sp[i].n;
+      outs[i] = sp[i].out;
+    }
+    unsigned char* d_blob;
+    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_blob), bytes, st_));
+    PDMK_CUDA(cudaMemcpyAsync(d_blob, blob.data(), bytes, cudaMemcpyHostToDevice, st_));
+    return d_blob;
+  };
+  auto reduce = [&](const std::vector<Chunked>& sp, const double2* pbase, int H, const unsigned char* d_blob,
+                    size_t off_meta, size_t off_out, cudaStream_t st) {
+    if (sp.empty()) return;
+    const int nbx = int(sp.size());
+    const int* d_meta = reinterpret_cast<const int*>(d_blob + off_meta);
+    double2* const* d_outs = reinterpret_cast<double2* const*>(d_blob + off_out);
+    dim3 grid(grid_for(H), unsigned(nbx));
+    k_reduce_chunks<<<grid, TPB, 0, st>>>(pbase, d_meta, d_meta + nbx, d_outs, H);
+    PDMK_LAUNCH_CHECK();
+  };
+  if (!aux_) {
+    PDMK_CUDA(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking));
+    PDMK_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+    PDMK_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
   }
+
+  // Root pass first, on the second stream: the root (node 0, all slots) needs
+  // no host view of the tree, so it runs while the host lays out the boxes.
+  // Its allocations are made on the tree's stream before the fork event.
+  const int nch_root = std::max(1, (D.n_slots + KSPLIT_ROOT - 1) / KSPLIT_ROOT);
+  std::vector<Chunked> root_split{{0, nch_root, D.out_root}};
+  double2* part_r = nullptr;
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part_r), sizeof(double2) * (size_t(nch_root) * D.Hw + 1), st_));
+  std::vector<NudftWork> wroot;
+  for (int c = 0; c < nch_root; ++c) {
+    int sb = c * KSPLIT_ROOT, se = std::min(D.n_slots, sb + KSPLIT_ROOT);
+    make_work(wroot, D.n_window, 0, 0, part_r + size_t(c) * D.Hw, sb, se);
+  }
+  double2* tab_root = nullptr;
+  std::vector<int2> ch_root;
+  plan_nudft_tables(D.n_window, wroot, &tab_root, ch_root, st_);
+  size_t rch, rmeta, rout;
+  unsigned char* d_root = upload(wroot, ch_root, root_split, &rch, &rmeta, &rout);
+  PDMK_CUDA(cudaEventRecord(ev_fork_, st_));
+  PDMK_CUDA(cudaStreamWaitEvent(aux_, ev_fork_, 0));
+  dispatch_nudft(D.n_window, reinterpret_cast<const NudftWork*>(d_root), int(wroot.size()),
+                 reinterpret_cast<const int2*>(d_root + rch), int(ch_root.size()), D, aux_);
+  reduce(root_split, part_r, D.Hw, d_root, rmeta, rout, aux_);
+  PDMK_CUDA(cudaEventRecord(ev_join_, aux_));
+
+  // host view of node slot ranges and coordinates for the box work list
+  // (and, on a new tree, of the children for the box lists: one round trip)
+  const int nn = D.n_nodes;
+  std::vector<int> nb(nn), ne(nn), lv(nn), c0;
+  std::vector<uint64_t> pf(nn);
+  PDMK_CUDA(cudaMemcpyAsync(nb.data(), D.node_begin, 4 * nn, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaMemcpyAsync(ne.data(), D.node_end, 4 * nn, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaMemcpyAsync(lv.data(), D.node_level, 4 * nn, cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaMemcpyAsync(pf.data(), D.node_prefix, 8 * nn, cudaMemcpyDeviceToHost, st_));
+  if (!box_lists_ready_) {
+    c0.resize(nn);
+    PDMK_CUDA(cudaMemcpyAsync(c0.data(), D.node_child0, 4 * nn, cudaMemcpyDeviceToHost, st_));
+  }
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  if (!box_lists_ready_) build_box_lists(c0);
+  struct Box {
+    int node, sb, se, level;
+    double2* out;
+  };
+  std::vector<Box> boxes;
+  const int base = D.level_start[D.pw_lo];
+  if (D.pw_hi >= D.pw_lo)
+    for (int id = base; id < D.level_start[D.pw_hi + 1]; ++id)
+      boxes.push_back({id, nb[id], ne[id], lv[id], D.out + size_t(id - base) * D.H});
   // boxes: largest first (longest-processing-time order), split when large
   std::vector<int> order(boxes.size());
   for (size_t i = 0; i < order.size(); ++i) order[i] = int(i);
   std::stable_sort(order.begin(), order.end(),
                    [&](int a, int b) { return boxes[a].se - boxes[a].sb > boxes[b].se - boxes[b].sb; });
+  std::vector<Chunked> box_split;
   long chunk_cursor = 0;
   for (int oi : order) {
     const Box& bx = boxes[oi];
@@ -917,19 +971,9 @@ void DmkTree::form_outgoing_pw() {
       chunk_cursor += nch;
     }
   }
-  part_box = chunk_cursor * D.H;
-  double2* part = nullptr;
-  size_t part_bytes = sizeof(double2) * size_t(part_root + part_box + 1);
-  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part), part_bytes, st_));
-  double2* part_b = part + part_root;
-  {
-    Box r{0, 0, D.n_slots, 0, D.out_root};
-    int nch = root_split[0].n;
-    for (int c = 0; c < nch; ++c) {
-      int sb = c * KSPLIT_ROOT, se = std::min(D.n_slots, sb + KSPLIT_ROOT);
-      make_work(wroot, D.n_window, r, part + size_t(c) * D.Hw, sb, se);
-    }
-  }
+  double2* part_b = nullptr;
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part_b), sizeof(double2) * (size_t(chunk_cursor) * D.H + 1), st_));
+  std::vector<NudftWork> wbox;
   {
     size_t si = 0;
     long cur = 0;
@@ -940,85 +984,30 @@ void DmkTree::form_outgoing_pw() {
         int nch = box_split[si].n;
         for (int c = 0; c < nch; ++c) {
           int sb = bx.sb + c * KSPLIT, se = std::min(bx.se, sb + KSPLIT);
-          make_work(wbox, D.n_diff, bx, part_b + size_t(cur + c) * D.H, sb, se);
+          make_work(wbox, D.n_diff, bx.level, pf[bx.node], part_b + size_t(cur + c) * D.H, sb, se);
         }
         cur += nch;
         ++si;
       } else {
-        make_work(wbox, D.n_diff, bx, bx.out, bx.sb, bx.se);
+        make_work(wbox, D.n_diff, bx.level, pf[bx.node], bx.out, bx.sb, bx.se);
       }
     }
   }
-  // factor tables of both passes (allocated here on st_, so the root pass on
-  // the second stream is ordered after the allocation by the fork event)
-  double2 *tab_box = nullptr, *tab_root = nullptr;
-  std::vector<int2> ch_box, ch_root;
+  double2* tab_box = nullptr;
+  std::vector<int2> ch_box;
   plan_nudft_tables(D.n_diff, wbox, &tab_box, ch_box, st_);
-  plan_nudft_tables(D.n_window, wroot, &tab_root, ch_root, st_);
-  // one upload: the work items (boxes first, then the root chunks), their
-  // table chunk lists, then per split-K group its first chunk, chunk count
-  // and output, for the reductions
-  const size_t nw = wroot.size() + wbox.size();
-  auto align16 = [](size_t b) { return (b + 15) & ~size_t(15); };
-  const size_t off_cbox = align16(sizeof(NudftWork) * nw);
-  const size_t off_croot = align16(off_cbox + sizeof(int2) * ch_box.size());
-  const size_t off_rmeta = align16(off_croot + sizeof(int2) * ch_root.size());
-  const size_t off_rout = align16(off_rmeta + sizeof(int) * 2 * root_split.size());
-  const size_t off_bmeta = align16(off_rout + sizeof(double2*) * root_split.size());
-  const size_t off_bout = align16(off_bmeta + sizeof(int) * 2 * box_split.size());
-  const size_t blob_bytes = align16(off_bout + sizeof(double2*) * box_split.size()) + 16;
-  std::vector<unsigned char> blob(blob_bytes, 0);
-  std::memcpy(blob.data(), wbox.data(), sizeof(NudftWork) * wbox.size());
-  std::memcpy(blob.data() + sizeof(NudftWork) * wbox.size(), wroot.data(), sizeof(NudftWork) * wroot.size());
-  std::memcpy(blob.data() + off_cbox, ch_box.data(), sizeof(int2) * ch_box.size());
-  std::memcpy(blob.data() + off_croot, ch_root.data(), sizeof(int2) * ch_root.size());
-  auto put_meta = [&](const std::vector<Chunked>& sp, size_t off_meta, size_t off_out) {
-    int* meta = reinterpret_cast<int*>(blob.data() + off_meta);
-    double2** outs = reinterpret_cast<double2**>(blob.data() + off_out);
-    for (size_t i = 0; i < sp.size(); ++i) {
-      meta[i] = sp[i].first;
-      meta[sp.size() + i] = sp[i].n;
-      outs[i] = sp[i].out;
-    }
-  };
-  put_meta(root_split, off_rmeta, off_rout);
-  put_meta(box_split, off_bmeta, off_bout);
-  unsigned char* d_blob;
-  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_blob), blob_bytes, st_));
-  PDMK_CUDA(cudaMemcpyAsync(d_blob, blob.data(), blob_bytes, cudaMemcpyHostToDevice, st_));
-  NudftWork* d_work = reinterpret_cast<NudftWork*>(d_blob);
-  // the root pass (few CTAs) overlaps the box pass on a second stream
-  if (!aux_) {
-    PDMK_CUDA(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking));
-    PDMK_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
-    PDMK_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
-  }
-  PDMK_CUDA(cudaEventRecord(ev_fork_, st_));
-  PDMK_CUDA(cudaStreamWaitEvent(aux_, ev_fork_, 0));
-  dispatch_nudft(D.n_window, d_work + wbox.size(), int(wroot.size()), reinterpret_cast<const int2*>(d_blob + off_croot),
-                 int(ch_root.size()), D, aux_);
-  PDMK_CUDA(cudaEventRecord(ev_join_, aux_));
+  size_t bch, bmeta, bout;
+  unsigned char* d_box = upload(wbox, ch_box, box_split, &bch, &bmeta, &bout);
   time_begin(3);
-  dispatch_nudft(D.n_diff, d_work, int(wbox.size()), reinterpret_cast<const int2*>(d_blob + off_cbox),
-                 int(ch_box.size()), D, st_);
+  dispatch_nudft(D.n_diff, reinterpret_cast<const NudftWork*>(d_box), int(wbox.size()),
+                 reinterpret_cast<const int2*>(d_box + bch), int(ch_box.size()), D, st_);
   time_end(3);
+  reduce(box_split, part_b, D.H, d_box, bmeta, bout, st_);
+  // the root pass's buffers are released after it joins the tree's stream
   PDMK_CUDA(cudaStreamWaitEvent(st_, ev_join_, 0));
-  // reduce split-K chunks
-  auto reduce = [&](const std::vector<Chunked>& sp, const double2* pbase, int H, size_t off_meta, size_t off_out) {
-    if (sp.empty()) return;
-    const int nbx = int(sp.size());
-    const int* d_meta = reinterpret_cast<const int*>(d_blob + off_meta);
-    double2* const* d_outs = reinterpret_cast<double2* const*>(d_blob + off_out);
-    dim3 grid(grid_for(H), unsigned(nbx));
-    k_reduce_chunks<<<grid, TPB, 0, st_>>>(pbase, d_meta, d_meta + nbx, d_outs, H);
-    PDMK_LAUNCH_CHECK();
-  };
-  reduce(root_split, part, D.Hw, off_rmeta, off_rout);
-  reduce(box_split, part_b, D.H, off_bmeta, off_bout);
-  PDMK_CUDA(cudaFreeAsync(d_blob, st_));
-  PDMK_CUDA(cudaFreeAsync(tab_box, st_));
-  PDMK_CUDA(cudaFreeAsync(tab_root, st_));
-  PDMK_CUDA(cudaFreeAsync(part, st_));
+  for (void* p : {static_cast<void*>(d_root), static_cast<void*>(tab_root), static_cast<void*>(part_r),
+                  static_cast<void*>(d_box), static_cast<void*>(tab_box), static_cast<void*>(part_b)})
+    PDMK_CUDA(cudaFreeAsync(p, st_));
   diff_cached_ = false;
 }
 
