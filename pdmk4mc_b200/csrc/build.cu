@@ -422,18 +422,6 @@ __global__ void k_validate(const double* r, const double* q, long n, double L, i
 
 }  // namespace
 
-bool device_positions_valid(const double* d_r, const double* d_q, long n, double L, cudaStream_t st) {
-  int* bad;
-  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&bad), 16, st));
-  PDMK_CUDA(cudaMemsetAsync(bad, 0, 4, st));
-  k_validate<<<grid_for(n), TPB, 0, st>>>(d_r, d_q, n, L, bad);
-  PDMK_LAUNCH_CHECK();
-  int h = 0;
-  PDMK_CUDA(cudaMemcpyAsync(&h, bad, 4, cudaMemcpyDeviceToHost, st));
-  PDMK_CUDA(cudaFreeAsync(bad, st));
-  PDMK_CUDA(cudaStreamSynchronize(st));
-  return h == 0;
-}
 
 // ---------------------------------------------------------------------------
 // Tree-lifetime allocations come from the device's stream-ordered pool, kept
@@ -517,6 +505,19 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
     PDMK_CUDA(cudaMemcpyAsync(r, r_in, size_t(3 * n) * sizeof(double), cudaMemcpyHostToDevice, st_));
     PDMK_CUDA(cudaMemcpyAsync(q, q_in, size_t(n) * sizeof(double), cudaMemcpyHostToDevice, st_));
   }
+  // refined cells per level (level 0: the root) and, in the last word, the
+  // count of invalid device inputs; read back together after the shallow
+  // refinement levels
+  constexpr int kBadWord = MAX_LEVEL + 2;
+  int* d_lvl;
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_lvl), sizeof(int) * (kBadWord + 1), st_));
+  PDMK_CUDA(cudaMemsetAsync(d_lvl, 0, sizeof(int) * (kBadWord + 1), st_));
+  if (on_device) {
+    // keys clamp every coordinate to the grid, so a build from invalid data
+    // stays in bounds until the check below rejects it
+    k_validate<<<grid_for(n), TPB, 0, st_>>>(r, q, n, L_, d_lvl + kBadWord);
+    PDMK_LAUNCH_CHECK();
+  }
   // keys, sort
   uint64_t* keys;
   int* ord;
@@ -550,10 +551,6 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
   put_small(lists[0], &zero, 8, st_);
   int maxref = 0;  // deepest level holding a refined cell
   {
-    // refined cells per level (level 0: the root), on the device
-    int* d_lvl;
-    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_lvl), sizeof(int) * (MAX_LEVEL + 2), st_));
-    PDMK_CUDA(cudaMemsetAsync(d_lvl, 0, sizeof(int) * (MAX_LEVEL + 2), st_));
     const int one = 1;
     put_small(d_lvl, &one, 4, st_);
     // root: refined (all nodes above level 2 are refined)
@@ -572,9 +569,16 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
     // read-back; deeper trees continue level by level
     constexpr int kEager = 6;
     for (int l = 1; l <= kEager; ++l) refine(l, grid_for(list_cap));
-    int cnt[MAX_LEVEL + 2] = {0};
-    PDMK_CUDA(cudaMemcpyAsync(cnt, d_lvl, sizeof(int) * (kEager + 1), cudaMemcpyDeviceToHost, st_));
+    int cnt[kBadWord + 1] = {0};
+    PDMK_CUDA(cudaMemcpyAsync(cnt, d_lvl, sizeof(cnt), cudaMemcpyDeviceToHost, st_));
     PDMK_CUDA(cudaStreamSynchronize(st_));
+    if (cnt[kBadWord] != 0) {
+      for (void* p : {static_cast<void*>(d_lvl), static_cast<void*>(keys), static_cast<void*>(ord), sort_scr,
+                      static_cast<void*>(dsx), static_cast<void*>(d_cnt), static_cast<void*>(lists[0]),
+                      static_cast<void*>(lists[1])})
+        PDMK_CUDA(cudaFreeAsync(p, st_));
+      throw BadInput("positions must lie in [0, L) and charges be finite");
+    }
     for (int l = 1; l <= kEager; ++l) {
       if (long(cnt[l - 1]) * 8 > list_cap || cnt[l] > list_cap)
         throw std::runtime_error("tree build: refinement list overflow");

@@ -83,6 +83,8 @@ int guarded(F&& f) {
     return f();
   } catch (const std::bad_alloc& e) {
     return fail(HPDMK_ERR_OUT_OF_MEMORY, e.what());
+  } catch (const pdmk::BadInput& e) {
+    return fail(HPDMK_ERR_BAD_INPUT, e.what());
   } catch (const pdmk::CudaError& e) {
     std::string m = e.what();
     if (m.find("out of memory") != std::string::npos) return fail(HPDMK_ERR_OUT_OF_MEMORY, m);
@@ -159,8 +161,6 @@ hpdmk_tree init_impl(HPDMKParams params, const HPDMKExtParams* ext, int n, const
     }
     hh->n = n;
     hh->L = params.L;
-    if (on_device && !pdmk::device_positions_valid(r, q, n, params.L, hh->stream))
-      return fail(HPDMK_ERR_BAD_INPUT, "positions must lie in [0, L) and charges be finite");
     hh->tree = std::make_unique<pdmk::DmkTree>(params.L, params.n_per_leaf, params.digits, n, r, q, on_device, opt,
                                                hh->stream);
     h = hh.release();

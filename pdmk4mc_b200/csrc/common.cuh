@@ -19,6 +19,11 @@ struct CudaError : std::runtime_error {
   explicit CudaError(const std::string& s) : std::runtime_error(s) {}
 };
 
+// invalid caller data found on the device (positions outside [0, L), charges not finite)
+struct BadInput : std::runtime_error {
+  explicit BadInput(const std::string& s) : std::runtime_error(s) {}
+};
+
 #define PDMK_CUDA(call)                                                                               \
   do {                                                                                                \
     cudaError_t err__ = (call);                                                                       \

@@ -169,8 +169,6 @@ struct EnergyParts {
   double total() const { return window + diff + res; }
 };
 
-// positions in [0, L) and finite charges, checked on the device (synchronises)
-bool device_positions_valid(const double* d_r, const double* d_q, long n, double L, cudaStream_t st);
 
 struct TreeOptions {
   int leaf_slack = 0;      // extra particle slots per leaf for moves

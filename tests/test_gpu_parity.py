@@ -68,6 +68,40 @@ def test_tree_bit_exact_deep():
     g.close()
 
 
+def test_device_inputs_rejected_then_accepted():
+    # positions already on the device are checked on the device during the
+    # build: outside [0, L) or a non-finite charge is HPDMK_ERR_BAD_INPUT, and
+    # a valid build afterwards gives the host-input tree's energy
+    import torch
+    L, n = 10.0, 2000
+    r, q = system("uniform", n, L, seed=3)
+    params = P.HPDMKParams(n_per_leaf=10, digits=6, L=L, init=P.DIRECT)
+    bad_r = r.copy()
+    bad_r[3 * 17 + 1] = L  # one coordinate at L, outside [0, L)
+    bad_q = q.copy()
+    bad_q[5] = np.nan
+    for rr, qq in ((bad_r, q), (r, bad_q)):
+        d_r = torch.tensor(rr, dtype=torch.float64, device="cuda")
+        d_q = torch.tensor(qq, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        with pytest.raises(P.HPDMKError) as e:
+            P.HPDMKPtTree(params, None, None, device_inputs=(d_r.data_ptr(), d_q.data_ptr(), n))
+        assert e.value.code == 2 and "positions must lie" in str(e.value)
+    d_r = torch.tensor(r, dtype=torch.float64, device="cuda")
+    d_q = torch.tensor(q, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    g = P.HPDMKPtTree(params, None, None, device_inputs=(d_r.data_ptr(), d_q.data_ptr(), n))
+    h = P.HPDMKPtTree(params, r, q)
+    try:
+        for t in (g, h):
+            t.form_outgoing_pw()
+            t.form_incoming_pw()
+        assert g.eval_energy() == h.eval_energy()
+    finally:
+        g.close()
+        h.close()
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_tree_bit_exact(case):
     g, o, r, q = pair(*case)
