@@ -700,17 +700,16 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
   PDMK_CUDA(cudaMemsetAsync(d_cnt, 0, 4, st_));
   k_collect_leaves<<<grid_for(n_nodes), TPB, 0, st_>>>(n_nodes, na.prefix, na.level, na.child0, lkey, lid, d_cnt);
   PDMK_LAUNCH_CHECK();
-  int nl = 0;
-  PDMK_CUDA(cudaMemcpyAsync(&nl, d_cnt, 4, cudaMemcpyDeviceToHost, st_));
-  PDMK_CUDA(cudaStreamSynchronize(st_));
+  // leaves = nodes less refined cells (the root and every refined cell of
+  // levels 1..maxref is exactly one non-leaf node), known without a read-back
+  int nl = n_nodes;
+  for (int l = 0; l <= maxref; ++l) nl -= refined[l];
   {
     void* scr;
     PDMK_CUDA(cudaMallocAsync(&scr, radix_sort_scratch_bytes(std::max(nl, 64)), st_));
     radix_sort_pairs(lkey, lid, nl, 8, scr, st_);
     PDMK_CUDA(cudaFreeAsync(scr, st_));
   }
-  leaf_ids_.assign(nl, 0);
-  PDMK_CUDA(cudaMemcpyAsync(leaf_ids_.data(), lid, sizeof(int) * nl, cudaMemcpyDeviceToHost, st_));
   int* cnt = static_cast<int*>(alloc(sizeof(int) * nl));
   int* cap = static_cast<int*>(alloc(sizeof(int) * nl));
   long* src_lo;

@@ -265,7 +265,6 @@ class DmkTree {
   DevTree dev_{};
   // host copies of the topology
   std::vector<int> h_level_start_;
-  std::vector<int> leaf_ids_;  // leaves in depth-first (Morton) order
   std::vector<void*> allocs_;
   void* alloc(size_t bytes);
   // leaves in depth-first order and their slot bookkeeping (device)
