@@ -98,8 +98,11 @@ hpdmk_tree hpdmk_tree_init(MPI_Comm comm, HPDMKParams params, int n_src, const d
 hpdmk_tree hpdmk_tree_init_ext(MPI_Comm comm, HPDMKParams params, const HPDMKExtParams *ext, int n_src,
                                const double *r_src, const double *charge);
 
-/* As hpdmk_tree_init_ext with d_r_src[3n] and d_charge[n] already in device memory
- * (positions are validated on the device). */
+/* As hpdmk_tree_init_ext with d_r_src[3n] and d_charge[n] already in device memory.
+ * Positions and charges are validated on the device during the build; a
+ * position outside [0, L) or a non-finite charge returns NULL with
+ * HPDMK_ERR_BAD_INPUT. The arrays are read on the tree's stream and are no
+ * longer needed once the call returns. */
 hpdmk_tree hpdmk_tree_init_device(MPI_Comm comm, HPDMKParams params, const HPDMKExtParams *ext, int n_src,
                                   const double *d_r_src, const double *d_charge);
 
