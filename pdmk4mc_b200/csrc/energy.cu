@@ -549,8 +549,8 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
   const int cnt = T.leaf_count[node];
   double e = 0;
   if (l >= 2 && cnt > chunk * RES_TCH) {
-    const double b = level_box(T, l);
-    const double b2 = b * b * (1.0 + 1e-14);  // sqrt only near or inside the cut-off
+    const double b = level_box(T, l), inv_b = 1.0 / b;
+    const double b2 = b * b * (1.0 + 1e-14);  // square roots only near or inside the cut-off
     const int tb = T.node_begin[node];
     if (threadIdx.x < 36) {
       const int src = threadIdx.x;
@@ -644,10 +644,10 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
               inb = r2b <= b2 && uslot[j2] != tslot;
             }
             if (ina || inb) {
-              const double ra = sqrt(ina ? r2a : 0.25 * b * b), rb = sqrt(inb ? r2b : 0.25 * b * b);
-              const double pa = poly(ra, b), pb = poly(rb, b);
-              if (ina && ra <= b) et += uq[js] * pa;
-              if (inb && rb <= b) et += uq[j2] * pb;
+              // from_r2 is zero at and beyond the cut-off
+              const double pa = poly.from_r2(ina ? r2a : 0.0, inv_b), pb = poly.from_r2(inb ? r2b : 0.0, inv_b);
+              et += uq[js] * pa;
+              if (j2 < ns) et += uq[j2] * pb;
             }
           }
       }

@@ -150,6 +150,18 @@ struct ResidualPoly {
     for (int i = 0; i < NP; ++i) v = fma(v, xs, c[i]);
     return v / r;
   }
+  // the same kernel from r^2 with one reciprocal square root in place of a
+  // square root and two divisions (inv_b = 1 / b); zero at r = 0 as above
+  __device__ double from_r2(double r2, double inv_b) const {
+    if (!(r2 > 0.0)) return 0.0;
+    const double ri = rsqrt(r2);
+    const double xs = (r2 * ri * inv_b - 0.5) * 2.0;
+    if (fabs(xs) >= 1.0) return 0.0;
+    double v = 0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) v = fma(v, xs, c[i]);
+    return v * ri;
+  }
   // d/dr of the residual kernel, P'(x) (2 / b) / r - P(x) / r^2 with x = 2 r / b - 1
   __device__ double deriv(double r, double b) const {
     const double xs = (r / b - 0.5) * 2.0;
