@@ -241,12 +241,14 @@ void launch_nudft(const NudftWork* d_work, int nwork, const int2* d_chunks, int 
   using S = NudftShape<NK>;
   constexpr int TAB_SMEM = S::KC * (2 * S::DP + NK + 1) * int(sizeof(double2));
   if (nwork == 0) return;
-  static bool attr = false;
-  if (!attr) {
+  // set once per process, and thread-safely: replica energies call this from
+  // several host threads
+  static const bool attr = [] {
     PDMK_CUDA(cudaFuncSetAttribute(k_nudft<NK>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
     PDMK_CUDA(cudaFuncSetAttribute(k_nudft_tables<NK>, cudaFuncAttributeMaxDynamicSharedMemorySize, TAB_SMEM));
-    attr = true;
-  }
+    return true;
+  }();
+  (void)attr;
   if (nchunks > 0) {
     k_nudft_tables<NK><<<unsigned(nchunks), S::KC * 6, TAB_SMEM, st>>>(d_work, d_chunks, T.sx, T.sy, T.sz, T.sq);
     PDMK_LAUNCH_CHECK();

@@ -28,6 +28,18 @@
 namespace pdmk {
 namespace {
 
+// Raises a kernel's dynamic shared-memory limit to at least `bytes`. The
+// limit belongs to the function (shared by every tree), only ever grows, and
+// is changed under a lock: trees may be driven from several host threads.
+void raise_smem_limit(const void* func, size_t bytes, size_t& limit) {
+  static std::mutex mu;
+  std::lock_guard<std::mutex> g(mu);
+  if (bytes > limit) {
+    PDMK_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    limit = bytes;
+  }
+}
+
 constexpr int SH_T = 256;
 constexpr int MAXLV = MAX_LEVELS;
 
@@ -1743,11 +1755,7 @@ void DmkTree::ensure_shift_config() {
     shift_grid_ = 2 + sms;
     const size_t smem = tables_smem(D, D.max_depth, 2);
     static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
-    const int slot = (D.n_poly - 7) / 6;
-    if (smem > smem_set[slot]) {
-      PDMK_CUDA(cudaFuncSetAttribute(shift_kernel(D.n_poly), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-      smem_set[slot] = smem;
-    }
+    raise_smem_limit(reinterpret_cast<const void*>(shift_kernel(D.n_poly)), smem, smem_set[(D.n_poly - 7) / 6]);
   }
 }
 
@@ -1903,11 +1911,7 @@ void DmkTree::mc_run_persistent(int n_moves, const int* d_idx, const double* d_d
     PDMK_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     if (!coop) throw CudaError("device does not support cooperative launches");
     static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
-    const int slot = (D.n_poly - 7) / 6;
-    if (smem > smem_set[slot]) {
-      PDMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-      smem_set[slot] = smem;
-    }
+    raise_smem_limit(reinterpret_cast<const void*>(kern), smem, smem_set[(D.n_poly - 7) / 6]);
     int per_sm = 0;
     PDMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, MC_T, smem));
     if (per_sm < 1) throw CudaError("persistent Metropolis kernel does not fit on one SM");
@@ -1989,11 +1993,7 @@ void DmkTree::shift_batch_device(int m, const int* d_idx, const double* d_disp, 
   const size_t smem = tables_smem(D, D.max_depth, 2);
   const ShiftBatchKernel kern = shift_batch_kernel(D.n_poly);
   static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
-  const int slot = (D.n_poly - 7) / 6;
-  if (smem > smem_set[slot]) {
-    PDMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    smem_set[slot] = smem;
-  }
+  raise_smem_limit(reinterpret_cast<const void*>(kern), smem, smem_set[(D.n_poly - 7) / 6]);
   const double pi = 3.14159265358979323846;
   const double c_window = std::pow(D.delta_k[0], 3) / std::pow(2 * pi, 3);
   kern<<<unsigned(m), SB_T, smem, st_>>>(D, d_idx, d_disp, c_window, d_dE);
@@ -2128,11 +2128,7 @@ void DmkTree::replicas_mc_run(const std::vector<DmkTree*>& ts, int m, const int*
   PDMK_CUDA(cudaMemcpyAsync(d_trees, hd.data(), sizeof(DevTree) * hd.size(), cudaMemcpyHostToDevice, st));
   const McRepKernel kern = mc_rep_kernel(np);
   static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function
-  const int slot = (np - 7) / 6;
-  if (smem > smem_set[slot]) {
-    PDMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    smem_set[slot] = smem;
-  }
+  raise_smem_limit(reinterpret_cast<const void*>(kern), smem, smem_set[(np - 7) / 6]);
   kern<<<unsigned(ts.size()), REP_T, smem, st>>>(d_trees, m, d_idx, d_disp, d_u, beta, d_dE, d_acc);
   PDMK_LAUNCH_CHECK();
   PDMK_CUDA(cudaFreeAsync(d_trees, st));
@@ -2155,11 +2151,7 @@ void DmkTree::potential_batch(int m, const int* d_idx, double* d_phi, double* d_
   const size_t smem = tables_smem(D, D.max_depth, 1);
   const PotentialKernel kern = potential_kernel(D.n_poly);
   static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
-  const int slot = (D.n_poly - 7) / 6;
-  if (smem > smem_set[slot]) {
-    PDMK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    smem_set[slot] = smem;
-  }
+  raise_smem_limit(reinterpret_cast<const void*>(kern), smem, smem_set[(D.n_poly - 7) / 6]);
   const double pi = 3.14159265358979323846;
   const double c_window = std::pow(D.delta_k[0], 3) / std::pow(2 * pi, 3);
   const double self_w = ps_.psi0_0 / (2 * D.boxsize[2] * ps_.C0);
