@@ -11,7 +11,9 @@
 //   out[(kz,ky), kx] = sum_j (q_j ez_j[kz] ey_j[ky]) ex_j[kx]
 // with box-centred coordinates: exp(-i k.x) = exp(-i k.c_B) exp(-i k.(x-c_B)),
 // where k.c_B is an exact multiple of pi/3 (k = m dk_l, dk_l bs_l = 2 pi / 3),
-// so the decentring factor is an exact sixth root of unity per axis.
+// so the decentring factor is an exact sixth root of unity per axis. A table
+// pass writes each work item's per-particle factors ex, ey, ez to HBM once;
+// the contraction streams them chunk by chunk into shared memory.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
