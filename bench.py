@@ -33,6 +33,7 @@ sys.path.insert(0, ROOT)
 METRIC = "MC trial moves/s & full-energy evals/s, mixed vs FP64 GPU at 1e-8 rel err"
 WORKLOAD = dict(workload="uniform periodic cube, Metropolis MC + full energy", N=100000, L=46.4, digits=9,
                 n_per_leaf=200, moves_per_step=10000, step=0.3, beta=1.0, charges="alternating +1/-1")
+WORKLOAD_N1E5 = WORKLOAD
 
 
 def make_system(seed, n, L):

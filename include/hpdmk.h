@@ -67,16 +67,25 @@ typedef void *hpdmk_tree;
 #define HPDMK_ERR_BAD_INPUT 2      /* n < 1, null pointer, position outside [0,L), non-finite value, index out of range */
 #define HPDMK_ERR_CUDA 4           /* CUDA runtime failure (message via hpdmk_last_error_message) */
 #define HPDMK_ERR_OUT_OF_MEMORY 5  /* device allocation failed */
-#define HPDMK_ERR_DEVICE 6         /* device-side error word set (overflow pool exhausted, grid barrier wait gave up) */
+#define HPDMK_ERR_DEVICE 6         /* device-side error word set (overflow pool exhausted, a bounded wait in a kernel gave up) */
 #define HPDMK_ERR_INTERNAL 7
 
-/* precision modes of hpdmk_tree_init_ext */
+/* precision modes of hpdmk_tree_init_ext.
+ * HPDMK_PRECISION_FP64: every step in FP64 (the drop-in path).
+ * HPDMK_PRECISION_MIXED: the outgoing plane-wave expansions (root and boxes,
+ * the reference's outgoing_pw_root / outgoing_pw_direct, src/planewave.cpp:24-84)
+ * are formed on the tensor cores from 8-bit integer slices of the phase
+ * factors (three 7-bit slices per operand, exact 32-bit integer sums,
+ * FP64 combination), a coefficient error near 1e-7 of the largest factor;
+ * the incoming expansions, energy sums, near field, energy shifts and updates
+ * stay FP64. */
 #define HPDMK_PRECISION_FP64 0
+#define HPDMK_PRECISION_MIXED 1
 
 typedef struct HPDMKExtParams {
   int leaf_slack;     /* free particle slots per leaf kept for moves (default 8) */
   int pool_capacity;  /* overflow slots for arrivals into full leaves (default 4096) */
-  int precision;      /* HPDMK_PRECISION_FP64 */
+  int precision;      /* HPDMK_PRECISION_FP64 (default) or HPDMK_PRECISION_MIXED */
   int device;         /* CUDA device ordinal (default 0) */
   void *stream;       /* cudaStream_t to run on; NULL: the tree creates its own */
 } HPDMKExtParams;

@@ -788,7 +788,9 @@ void DmkTree::layout_slots(const double* dsx, const double* dsy, const double* d
   if (n_slots > slot_capacity_) {
     // slot arrays live outside allocs_ so they can be regrown
     if (slot_block_) cudaFreeAsync(slot_block_, st_);
-    slot_capacity_ = n_slots + n_slots / 8 + 64;
+    // a multiple of 32 slots: the mixed pass reads the four slot arrays as
+    // one 2-D tensor (TMA row strides must be multiples of 16 bytes)
+    slot_capacity_ = (n_slots + n_slots / 8 + 64 + 31) & ~31;
     PDMK_CUDA(cudaMallocAsync(&slot_block_, size_t(slot_capacity_) * (4 * sizeof(double) + sizeof(int)), st_));
   }
   double* base = static_cast<double*>(slot_block_);

@@ -85,6 +85,8 @@ int guarded(F&& f) {
     return fail(HPDMK_ERR_OUT_OF_MEMORY, e.what());
   } catch (const pdmk::BadInput& e) {
     return fail(HPDMK_ERR_BAD_INPUT, e.what());
+  } catch (const pdmk::DeviceError& e) {
+    return fail(HPDMK_ERR_DEVICE, e.what());
   } catch (const pdmk::CudaError& e) {
     std::string m = e.what();
     if (m.find("out of memory") != std::string::npos) return fail(HPDMK_ERR_OUT_OF_MEMORY, m);
@@ -97,6 +99,22 @@ int guarded(F&& f) {
 }
 
 Handle* H(hpdmk_tree t) { return static_cast<Handle*>(t); }
+
+// Makes the tree's device current for one call and restores the caller's
+// device afterwards: every tree's stream, buffers and kernel attributes
+// belong to the device it was created on.
+struct DeviceGuard {
+  int prev = -1, want = 0;
+  explicit DeviceGuard(int dev) : want(dev) {
+    PDMK_CUDA(cudaGetDevice(&prev));
+    if (prev != want) PDMK_CUDA(cudaSetDevice(want));
+  }
+  ~DeviceGuard() {
+    if (prev >= 0 && prev != want) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
 
 // device error word: bit 0 overflow pool exhausted, bit 1 grid barrier wait gave up
 int device_fail(int e) {
@@ -145,14 +163,18 @@ hpdmk_tree init_impl(HPDMKParams params, const HPDMKExtParams* ext, int n, const
   }
   Handle* h = nullptr;
   int st = guarded([&]() {
+    // the guard outlives the handle under construction, so a failed build
+    // releases its device memory with its own device current
+    DeviceGuard dg(ext ? ext->device : 0);
     auto hh = std::make_unique<Handle>();
     pdmk::TreeOptions opt;
     opt.leaf_slack = ext ? ext->leaf_slack : 8;
     opt.pool_capacity = ext && ext->pool_capacity > 0 ? ext->pool_capacity : 4096;
     if (opt.leaf_slack < 0) return fail(HPDMK_ERR_BAD_PARAMS, "leaf_slack must be >= 0");
-    if (ext && ext->precision != HPDMK_PRECISION_FP64) return fail(HPDMK_ERR_BAD_PARAMS, "unknown precision mode");
+    if (ext && ext->precision != HPDMK_PRECISION_FP64 && ext->precision != HPDMK_PRECISION_MIXED)
+      return fail(HPDMK_ERR_BAD_PARAMS, "unknown precision mode");
+    opt.precision = ext ? ext->precision : HPDMK_PRECISION_FP64;
     hh->device = ext ? ext->device : 0;
-    PDMK_CUDA(cudaSetDevice(hh->device));
     if (ext && ext->stream) {
       hh->stream = static_cast<cudaStream_t>(ext->stream);
       hh->own_stream = false;
@@ -193,12 +215,19 @@ hpdmk_tree hpdmk_tree_init_device(MPI_Comm, HPDMKParams params, const HPDMKExtPa
 }
 
 void hpdmk_tree_destroy(hpdmk_tree tree) {
-  if (tree) delete H(tree);
+  if (!tree) return;
+  try {
+    DeviceGuard dg(H(tree)->device);
+    delete H(tree);
+  } catch (...) {
+    delete H(tree);  // the device could not be made current: release what can be released
+  }
 }
 
 int hpdmk_form_outgoing_pw(hpdmk_tree t) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->form_outgoing_pw();
     return ok();
   });
@@ -207,6 +236,7 @@ int hpdmk_form_outgoing_pw(hpdmk_tree t) {
 int hpdmk_form_incoming_pw(hpdmk_tree t) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->form_incoming_pw();
     return ok();
   });
@@ -215,6 +245,7 @@ int hpdmk_form_incoming_pw(hpdmk_tree t) {
 int hpdmk_eval_energy(hpdmk_tree t, double* energy, double* window, double* difference, double* residual) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     pdmk::EnergyParts p = H(t)->tree->eval_energy();
     if (energy) *energy = p.total();
     if (window) *window = p.window;
@@ -227,6 +258,7 @@ int hpdmk_eval_energy(hpdmk_tree t, double* energy, double* window, double* diff
 int hpdmk_energy(hpdmk_tree t, double* energy) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     auto* tr = H(t)->tree.get();
     tr->form_outgoing_pw();
     tr->form_incoming_pw();
@@ -240,6 +272,7 @@ int hpdmk_eval_shift_energy(hpdmk_tree t, long i, double dx, double dy, double d
   if (!t || !dE) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
   if (check_move(H(t), i, dx, dy, dz) != HPDMK_OK) return g_last_error;
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     *dE = H(t)->tree->eval_shift_energy(i, dx, dy, dz, nullptr);
     return ok();
   });
@@ -249,6 +282,7 @@ int hpdmk_debug_shift_parts(hpdmk_tree t, long i, double dx, double dy, double d
   if (!t || !parts) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
   if (check_move(H(t), i, dx, dy, dz) != HPDMK_OK) return g_last_error;
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->eval_shift_energy(i, dx, dy, dz, parts);
     return ok();
   });
@@ -258,6 +292,7 @@ int hpdmk_update_shift(hpdmk_tree t, long i, double dx, double dy, double dz) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   if (check_move(H(t), i, dx, dy, dz) != HPDMK_OK) return g_last_error;
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->update_shift(i, dx, dy, dz);
     if (int e = H(t)->tree->check_device_error()) return device_fail(e);
     return ok();
@@ -275,17 +310,9 @@ int hpdmk_eval_shift_energy_batch_static(hpdmk_tree t, int m, const long* i, con
     if (check_move(h, i[c], d[3 * c], d[3 * c + 1], d[3 * c + 2]) != HPDMK_OK) return g_last_error;
   if (m == 0) return ok();
   return guarded([&]() {
-    // the scratch address is per device: make the tree's device current
-    int prev = 0;
-    PDMK_CUDA(cudaGetDevice(&prev));
-    if (prev != h->device) PDMK_CUDA(cudaSetDevice(h->device));
-    try {
-      h->tree->shift_batch_static(m, i, d, dE);
-    } catch (...) {
-      if (prev != h->device) cudaSetDevice(prev);
-      throw;
-    }
-    if (prev != h->device) PDMK_CUDA(cudaSetDevice(prev));
+    // the static array's address is per device: the tree's device is current
+    DeviceGuard dg(h->device);
+    h->tree->shift_batch_static(m, i, d, dE);
     return ok();
   });
 }
@@ -297,6 +324,7 @@ int hpdmk_eval_shift_energy_batch(hpdmk_tree t, int m, const long* i, const doub
     if (check_move(h, i[c], d[3 * c], d[3 * c + 1], d[3 * c + 2]) != HPDMK_OK) return g_last_error;
   if (m == 0) return ok();
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     h->ensure(m);
     std::vector<int> ii(i, i + m);
     PDMK_CUDA(cudaMemcpyAsync(h->d_i, ii.data(), sizeof(int) * m, cudaMemcpyHostToDevice, h->stream));
@@ -316,6 +344,7 @@ int hpdmk_mc_run(hpdmk_tree t, int n, const long* i, const double* d, const doub
     if (check_move(h, i[c], d[3 * c], d[3 * c + 1], d[3 * c + 2]) != HPDMK_OK) return g_last_error;
   if (n == 0) return ok();
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     h->ensure(n);
     std::vector<int> ii(i, i + n);
     PDMK_CUDA(cudaMemcpyAsync(h->d_i, ii.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
@@ -335,6 +364,7 @@ int hpdmk_mc_run_device(hpdmk_tree t, int n, const int* d_i, const double* d_d, 
                         double* d_dE, int* d_accepted) {
   if (!t || n < 0 || (n > 0 && (!d_i || !d_d || !d_u))) return fail(HPDMK_ERR_BAD_INPUT, "bad move arguments");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->reset_work();
     H(t)->tree->mc_run_device(n, d_i, d_d, d_u, beta, d_dE, d_accepted);
     return ok();
@@ -344,6 +374,7 @@ int hpdmk_mc_run_device(hpdmk_tree t, int n, const int* d_i, const double* d_d, 
 int hpdmk_get_positions(hpdmk_tree t, double* r) {
   if (!t || !r) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->export_positions(r);
     return ok();
   });
@@ -363,6 +394,7 @@ int hpdmk_tree_info(hpdmk_tree t, long* info) {
 int hpdmk_synchronize(hpdmk_tree t) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->synchronize();
     return ok();
   });
@@ -390,6 +422,7 @@ int hpdmk_set_timing(hpdmk_tree t, int enable) {
 int hpdmk_get_timing(hpdmk_tree t, double* out, int reset) {
   if (!t || !out) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->get_timing(out, reset != 0);
     return ok();
   });
@@ -402,6 +435,7 @@ int hpdmk_eval_potential(hpdmk_tree t, int m, const long* i, double* phi, double
     if (i[c] < 0 || i[c] >= h->n) return fail(HPDMK_ERR_BAD_INPUT, "particle index out of range");
   if (m == 0) return ok();
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     h->ensure(m);
     std::vector<int> ii(i, i + m);
     double* d_field = nullptr;
@@ -436,6 +470,7 @@ int hpdmk_replicas_mc_run(int n_trees, const hpdmk_tree* trees, int m, const lon
   if (m == 0) return ok();
   Handle* h0 = H(trees[0]);
   return guarded([&]() {
+    DeviceGuard dg(h0->device);
     const size_t tot = size_t(n_trees) * m;
     std::vector<int> ii(i, i + tot);
     char* buf = nullptr;
@@ -496,6 +531,7 @@ int hpdmk_tree_rebuild(hpdmk_tree t) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   Handle* h = H(t);
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     const pdmk::DmkTree& old = *h->tree;
     const long n = old.n_particles();
     double* d_r = nullptr;
@@ -521,6 +557,7 @@ int hpdmk_tree_rebuild(hpdmk_tree t) {
 int hpdmk_ewald_energy(hpdmk_tree t, double* energy, double* parts) {
   if (!t || !energy) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     *energy = H(t)->tree->ewald_energy(parts);
     return ok();
   });
@@ -535,6 +572,7 @@ int hpdmk_get_launch_count(long long* out) {
 int hpdmk_get_update_bytes(hpdmk_tree t, double* out) {
   if (!t || !out) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->get_work(out);
     return ok();
   });
@@ -546,6 +584,7 @@ const char* hpdmk_last_error_message(void) { return g_last_message.c_str(); }
 int hpdmk_debug_nodes(hpdmk_tree t, int* level, unsigned long long* prefix, int* is_leaf, long* count) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->export_nodes(level, reinterpret_cast<uint64_t*>(prefix), is_leaf, count);
     return ok();
   });
@@ -554,6 +593,7 @@ int hpdmk_debug_nodes(hpdmk_tree t, int* level, unsigned long long* prefix, int*
 int hpdmk_debug_neighbors(hpdmk_tree t, int* col27, int* coarse8) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->export_neighbors(col27, coarse8);
     return ok();
   });
@@ -562,6 +602,7 @@ int hpdmk_debug_neighbors(hpdmk_tree t, int* col27, int* coarse8) {
 int hpdmk_debug_sorted_order(hpdmk_tree t, long* o) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->export_sorted_order(o);
     return ok();
   });
@@ -570,6 +611,7 @@ int hpdmk_debug_sorted_order(hpdmk_tree t, long* o) {
 int hpdmk_debug_pw(hpdmk_tree t, long node, int which, double* out) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     H(t)->tree->export_pw(node, which, out);
     return ok();
   });
@@ -578,6 +620,7 @@ int hpdmk_debug_pw(hpdmk_tree t, long node, int which, double* out) {
 int hpdmk_debug_kernels(hpdmk_tree t, int level, double* out) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
     if (level == 0) H(t)->tree->export_W(out);
     else H(t)->tree->export_D(level, out);
     return ok();

@@ -6,8 +6,11 @@
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 namespace pdmk {
 
@@ -17,6 +20,11 @@ constexpr int MAX_LEVELS = MAX_LEVEL + 1;
 
 struct CudaError : std::runtime_error {
   explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+
+// a device-side error word was set (a bounded wait in a kernel gave up)
+struct DeviceError : std::runtime_error {
+  explicit DeviceError(const std::string& s) : std::runtime_error(s) {}
 };
 
 // invalid caller data found on the device (positions outside [0, L), charges not finite)
@@ -34,6 +42,24 @@ struct BadInput : std::runtime_error {
 
 // kernels this library has launched (graph-executed ones included)
 inline std::atomic<long long> g_launch_count{0};
+
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`. The attribute belongs to the function in the current
+// device's context, so the limit already set is remembered per (function,
+// device); it only ever grows, under a lock (trees may be driven from several
+// host threads and live on different devices).
+inline void raise_smem_limit(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> set;
+  int dev = 0;
+  PDMK_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  size_t& limit = set[{func, dev}];
+  if (bytes > limit) {
+    PDMK_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    limit = bytes;
+  }
+}
 
 #define PDMK_LAUNCH_CHECK()                                  \
   do {                                                       \

@@ -17,9 +17,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
+#include "mixed.hpp"
 #include "tree.hpp"
 
 namespace pdmk {
@@ -243,14 +245,9 @@ void launch_nudft(const NudftWork* d_work, int nwork, const int2* d_chunks, int 
   using S = NudftShape<NK>;
   constexpr int TAB_SMEM = S::KC * (2 * S::DP + NK + 1) * int(sizeof(double2));
   if (nwork == 0) return;
-  // set once per process, and thread-safely: replica energies call this from
-  // several host threads
-  static const bool attr = [] {
-    PDMK_CUDA(cudaFuncSetAttribute(k_nudft<NK>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
-    PDMK_CUDA(cudaFuncSetAttribute(k_nudft_tables<NK>, cudaFuncAttributeMaxDynamicSharedMemorySize, TAB_SMEM));
-    return true;
-  }();
-  (void)attr;
+  // per device and thread-safe: replica energies call this from several host threads
+  raise_smem_limit(reinterpret_cast<const void*>(k_nudft<NK>), S::SMEM);
+  raise_smem_limit(reinterpret_cast<const void*>(k_nudft_tables<NK>), TAB_SMEM);
   if (nchunks > 0) {
     k_nudft_tables<NK><<<unsigned(nchunks), S::KC * 6, TAB_SMEM, st>>>(d_work, d_chunks, T.sx, T.sy, T.sz, T.sq);
     PDMK_LAUNCH_CHECK();
@@ -871,17 +868,54 @@ void DmkTree::form_outgoing_pw() {
       wl.push_back(w);
     }
   };
+  // the mixed pass: one item per (box or box chunk, pair of 128-row M tiles)
+  auto make_mix = [&](std::vector<MixItem>& wl, int nk, int l, uint64_t p, double2* out, int sb, int se) {
+    MixItem w{};
+    double scale = std::ldexp(1.0, -l);
+    int X = int(compact3(p)), Y = int(compact3(p >> 1)), Z = int(compact3(p >> 2));
+    w.cx = L_ * (double(X) * scale + 0.5 * scale);
+    w.cy = L_ * (double(Y) * scale + 0.5 * scale);
+    w.cz = L_ * (double(Z) * scale + 0.5 * scale);
+    w.dk = D.delta_k[l];
+    w.X = X;
+    w.Y = Y;
+    w.Z = Z;
+    w.M = l == 0 ? 3 : 1;
+    w.s_begin = sb;
+    w.s_end = se;
+    w.out = out;
+    const int pairs = mixed_pairs(nk);
+    for (int t = 0; t < pairs; ++t) {
+      w.pair = t;
+      wl.push_back(w);
+    }
+  };
+  const bool mixed = opt_.precision == 1;
+  CUtensorMap tmap{};
+  if (mixed) {
+    if (!d_mix_) {
+      d_mix_ = static_cast<double*>(alloc(sizeof(double) * 2));
+      PDMK_CUDA(cudaMemsetAsync(d_mix_, 0, sizeof(double) * 2, st_));
+    }
+    if (!qmax_ready_) {
+      launch_absmax(D.sq, D.n_slots, d_mix_, st_);
+      qmax_ready_ = true;
+    }
+    make_coord_map(&tmap, D.sx, slot_capacity_);
+  }
+  int* d_mix_err = mixed ? reinterpret_cast<int*>(d_mix_ + 1) : nullptr;
   auto align16 = [](size_t b) { return (b + 15) & ~size_t(15); };
   // one upload per pass: the work items, their table chunk lists, then per
   // split-K group its first chunk, chunk count and output
-  auto upload = [&](const std::vector<NudftWork>& wl, const std::vector<int2>& ch, const std::vector<Chunked>& sp,
-                    size_t* off_ch, size_t* off_meta, size_t* off_out) {
-    *off_ch = align16(sizeof(NudftWork) * wl.size());
+  auto upload = [&](const auto& wl, const std::vector<int2>& ch, const std::vector<Chunked>& sp, size_t* off_ch,
+                    size_t* off_meta, size_t* off_out) {
+    using Item = typename std::decay_t<decltype(wl)>::value_type;
+    *off_ch = align16(sizeof(Item) * wl.size());
     *off_meta = align16(*off_ch + sizeof(int2) * ch.size());
     *off_out = align16(*off_meta + sizeof(int) * 2 * sp.size());
     const size_t bytes = align16(*off_out + sizeof(double2*) * sp.size()) + 16;
     std::vector<unsigned char> blob(bytes, 0);
-    std::memcpy(blob.data(), wl.data(), sizeof(NudftWork) * wl.size());
+    std::memcpy(blob.data(), wl.data(), sizeof(Item) * wl.size());
     std::memcpy(blob.data() + *off_ch, ch.data(), sizeof(int2) * ch.size());
     int* meta = reinterpret_cast<int*>(blob.data() + *off_meta);
     double2** outs = reinterpret_cast<double2**>(blob.data() + *off_out);
@@ -919,19 +953,30 @@ void DmkTree::form_outgoing_pw() {
   double2* part_r = nullptr;
   PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part_r), sizeof(double2) * (size_t(nch_root) * D.Hw + 1), st_));
   std::vector<NudftWork> wroot;
+  std::vector<MixItem> mroot;
   for (int c = 0; c < nch_root; ++c) {
     int sb = c * KSPLIT_ROOT, se = std::min(D.n_slots, sb + KSPLIT_ROOT);
-    make_work(wroot, D.n_window, 0, 0, part_r + size_t(c) * D.Hw, sb, se);
+    if (mixed) make_mix(mroot, D.n_window, 0, 0, part_r + size_t(c) * D.Hw, sb, se);
+    else make_work(wroot, D.n_window, 0, 0, part_r + size_t(c) * D.Hw, sb, se);
   }
   double2* tab_root = nullptr;
   std::vector<int2> ch_root;
-  plan_nudft_tables(D.n_window, wroot, &tab_root, ch_root, st_);
   size_t rch, rmeta, rout;
-  unsigned char* d_root = upload(wroot, ch_root, root_split, &rch, &rmeta, &rout);
+  unsigned char* d_root = nullptr;
+  if (mixed) {
+    d_root = upload(mroot, ch_root, root_split, &rch, &rmeta, &rout);
+  } else {
+    plan_nudft_tables(D.n_window, wroot, &tab_root, ch_root, st_);
+    d_root = upload(wroot, ch_root, root_split, &rch, &rmeta, &rout);
+  }
   PDMK_CUDA(cudaEventRecord(ev_fork_, st_));
   PDMK_CUDA(cudaStreamWaitEvent(aux_, ev_fork_, 0));
-  dispatch_nudft(D.n_window, reinterpret_cast<const NudftWork*>(d_root), int(wroot.size()),
-                 reinterpret_cast<const int2*>(d_root + rch), int(ch_root.size()), D, aux_);
+  if (mixed)
+    dispatch_mixed(D.n_window, tmap, reinterpret_cast<const MixItem*>(d_root), int(mroot.size()), d_mix_, d_mix_err,
+                   aux_);
+  else
+    dispatch_nudft(D.n_window, reinterpret_cast<const NudftWork*>(d_root), int(wroot.size()),
+                   reinterpret_cast<const int2*>(d_root + rch), int(ch_root.size()), D, aux_);
   reduce(root_split, part_r, D.Hw, d_root, rmeta, rout, aux_);
   PDMK_CUDA(cudaEventRecord(ev_join_, aux_));
 
@@ -978,9 +1023,14 @@ void DmkTree::form_outgoing_pw() {
   double2* part_b = nullptr;
   PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part_b), sizeof(double2) * (size_t(chunk_cursor) * D.H + 1), st_));
   std::vector<NudftWork> wbox;
+  std::vector<MixItem> mbox;
   {
     size_t si = 0;
     long cur = 0;
+    auto add = [&](int l, uint64_t p, double2* out, int sb, int se) {
+      if (mixed) make_mix(mbox, D.n_diff, l, p, out, sb, se);
+      else make_work(wbox, D.n_diff, l, p, out, sb, se);
+    };
     for (int oi : order) {
       const Box& bx = boxes[oi];
       int cntp = bx.se - bx.sb;
@@ -988,30 +1038,39 @@ void DmkTree::form_outgoing_pw() {
         int nch = box_split[si].n;
         for (int c = 0; c < nch; ++c) {
           int sb = bx.sb + c * KSPLIT, se = std::min(bx.se, sb + KSPLIT);
-          make_work(wbox, D.n_diff, bx.level, pf[bx.node], part_b + size_t(cur + c) * D.H, sb, se);
+          add(bx.level, pf[bx.node], part_b + size_t(cur + c) * D.H, sb, se);
         }
         cur += nch;
         ++si;
       } else {
-        make_work(wbox, D.n_diff, bx.level, pf[bx.node], bx.out, bx.sb, bx.se);
+        add(bx.level, pf[bx.node], bx.out, bx.sb, bx.se);
       }
     }
   }
   double2* tab_box = nullptr;
   std::vector<int2> ch_box;
-  plan_nudft_tables(D.n_diff, wbox, &tab_box, ch_box, st_);
   size_t bch, bmeta, bout;
-  unsigned char* d_box = upload(wbox, ch_box, box_split, &bch, &bmeta, &bout);
+  unsigned char* d_box = nullptr;
+  if (mixed) {
+    d_box = upload(mbox, ch_box, box_split, &bch, &bmeta, &bout);
+  } else {
+    plan_nudft_tables(D.n_diff, wbox, &tab_box, ch_box, st_);
+    d_box = upload(wbox, ch_box, box_split, &bch, &bmeta, &bout);
+  }
   time_begin(3);
-  dispatch_nudft(D.n_diff, reinterpret_cast<const NudftWork*>(d_box), int(wbox.size()),
-                 reinterpret_cast<const int2*>(d_box + bch), int(ch_box.size()), D, st_);
+  if (mixed)
+    dispatch_mixed(D.n_diff, tmap, reinterpret_cast<const MixItem*>(d_box), int(mbox.size()), d_mix_, d_mix_err,
+                   st_);
+  else
+    dispatch_nudft(D.n_diff, reinterpret_cast<const NudftWork*>(d_box), int(wbox.size()),
+                   reinterpret_cast<const int2*>(d_box + bch), int(ch_box.size()), D, st_);
   time_end(3);
   reduce(box_split, part_b, D.H, d_box, bmeta, bout, st_);
   // the root pass's buffers are released after it joins the tree's stream
   PDMK_CUDA(cudaStreamWaitEvent(st_, ev_join_, 0));
   for (void* p : {static_cast<void*>(d_root), static_cast<void*>(tab_root), static_cast<void*>(part_r),
                   static_cast<void*>(d_box), static_cast<void*>(tab_box), static_cast<void*>(part_b)})
-    PDMK_CUDA(cudaFreeAsync(p, st_));
+    if (p) PDMK_CUDA(cudaFreeAsync(p, st_));
   diff_cached_ = false;
 }
 
@@ -1157,6 +1216,14 @@ double DmkTree::eval_res_energy() {
   return e;
 }
 
+int DmkTree::check_mixed_error() {
+  if (!d_mix_) return 0;
+  int e = 0;
+  PDMK_CUDA(cudaMemcpyAsync(&e, d_mix_ + 1, sizeof(int), cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  return e;
+}
+
 EnergyParts DmkTree::eval_energy() {
   // per-box charge sums and the near field read particles from the slot
   // ranges: fold any overflow-pool arrivals back into them first. The three
@@ -1166,8 +1233,11 @@ EnergyParts DmkTree::eval_energy() {
   if (!diff_cached_) run_incoming(false);
   launch_res_energy();
   double e[3];
+  int mix_err = 0;
   PDMK_CUDA(cudaMemcpyAsync(e, d_scalars_, sizeof(e), cudaMemcpyDeviceToHost, st_));
+  if (d_mix_) PDMK_CUDA(cudaMemcpyAsync(&mix_err, d_mix_ + 1, sizeof(int), cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaStreamSynchronize(st_));
+  if (mix_err) throw DeviceError("mixed-precision outgoing pass: a pipeline wait gave up");
   EnergyParts p;
   p.window = e[0];
   p.diff = e[1];

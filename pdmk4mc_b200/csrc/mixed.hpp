@@ -1,0 +1,32 @@
+// Host interface of the mixed-precision (tcgen05, int8-sliced) outgoing
+// plane-wave pass, mixed.cu.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+namespace pdmk {
+
+// One CTA of the mixed pass: M tiles `pair` (rows [pair * rows per CTA, ...))
+// of one box, or of one split-K chunk of a box, over the slots [s_begin, s_end).
+struct MixItem {
+  double cx, cy, cz;  // box centre
+  double dk;          // mode spacing of the box's level
+  int X, Y, Z;        // integer box coordinates at its level
+  int M;              // decentring multiplier: 1 for levels >= 2, 3 for the root
+  int s_begin, s_end;
+  int pair;
+  int pad_;
+  double2* out;  // the box's H complex outputs (or its split-K partial)
+};
+
+// CTAs per box for n modes per axis half
+int mixed_pairs(int nk);
+// 2-D tensor map over the slot arrays x, y, z, q (stride slot_capacity, which must be even)
+void make_coord_map(CUtensorMap* map, const double* sx, int slot_capacity);
+// max |q| over n charges into *out (one block)
+void launch_absmax(const double* sq, int n, double* out, cudaStream_t st);
+// one launch of the mixed pass over nitems device-resident items
+void dispatch_mixed(int nk, const CUtensorMap& tmap, const MixItem* d_items, int nitems, const double* d_qmax,
+                    int* d_err, cudaStream_t st);
+
+}  // namespace pdmk

@@ -28,18 +28,6 @@
 namespace pdmk {
 namespace {
 
-// Raises a kernel's dynamic shared-memory limit to at least `bytes`. The
-// limit belongs to the function (shared by every tree), only ever grows, and
-// is changed under a lock: trees may be driven from several host threads.
-void raise_smem_limit(const void* func, size_t bytes, size_t& limit) {
-  static std::mutex mu;
-  std::lock_guard<std::mutex> g(mu);
-  if (bytes > limit) {
-    PDMK_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
-    limit = bytes;
-  }
-}
-
 constexpr int SH_T = 256;
 constexpr int MAXLV = MAX_LEVELS;
 
@@ -1754,8 +1742,7 @@ void DmkTree::ensure_shift_config() {
     PDMK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     shift_grid_ = 2 + sms;
     const size_t smem = tables_smem(D, D.max_depth, 2);
-    static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
-    raise_smem_limit(reinterpret_cast<const void*>(shift_kernel(D.n_poly)), smem, smem_set[(D.n_poly - 7) / 6]);
+    raise_smem_limit(reinterpret_cast<const void*>(shift_kernel(D.n_poly)), smem);
   }
 }
 
@@ -1910,8 +1897,7 @@ void DmkTree::mc_run_persistent(int n_moves, const int* d_idx, const double* d_d
     PDMK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     PDMK_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     if (!coop) throw CudaError("device does not support cooperative launches");
-    static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
-    raise_smem_limit(reinterpret_cast<const void*>(kern), smem, smem_set[(D.n_poly - 7) / 6]);
+    raise_smem_limit(reinterpret_cast<const void*>(kern), smem);
     int per_sm = 0;
     PDMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, MC_T, smem));
     if (per_sm < 1) throw CudaError("persistent Metropolis kernel does not fit on one SM");
@@ -1992,8 +1978,7 @@ void DmkTree::shift_batch_device(int m, const int* d_idx, const double* d_disp, 
   if (m <= 0) return;
   const size_t smem = tables_smem(D, D.max_depth, 2);
   const ShiftBatchKernel kern = shift_batch_kernel(D.n_poly);
-  static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
-  raise_smem_limit(reinterpret_cast<const void*>(kern), smem, smem_set[(D.n_poly - 7) / 6]);
+  raise_smem_limit(reinterpret_cast<const void*>(kern), smem);
   const double pi = 3.14159265358979323846;
   const double c_window = std::pow(D.delta_k[0], 3) / std::pow(2 * pi, 3);
   kern<<<unsigned(m), SB_T, smem, st_>>>(D, d_idx, d_disp, c_window, d_dE);
@@ -2004,26 +1989,23 @@ void DmkTree::shift_batch_device(int m, const int* d_idx, const double* d_disp, 
 
 // ---------------------------------------------------------------------------
 // Candidate batch through a fixed static device buffer. For callers that may
-// not allocate device memory once the tree exists (a pool-managed process, a
-// host thread that must not enter the allocator between steps): the block
-// partials, completion counter, proposal record, phase tables and the staged
-// inputs/outputs all live in g_static_scratch, whose address is looked up once
-// per device. The completion counter must be zero when a launch starts: each
-// call clears it, and every launch's last block sets it back to zero.
+// not allocate device memory once the tree exists (a process that budgets its
+// device memory up front, a host thread that must not enter the allocator
+// between steps): the candidates' indices and displacements are staged into
+// g_static_scratch and their energy shifts come back through it, and the
+// batch is the same single launch of k_shift_batch as the allocating batch
+// (one block per candidate; its phase tables live in shared memory). The
+// array's device address is looked up once per device, with that device
+// current. Nothing in the buffer has to start at zero: every call writes the
+// inputs it reads, and the kernel writes every output before it is read.
 // Calls that overlap in time on one device (two host threads, two trees on
 // different streams) share the buffer and race; serialise them.
 namespace {
-constexpr int kStaticMaxMoves = 4096;   // candidates per call
-constexpr int kStaticMaxBlocks = 1024;  // shift grid (2 + SM count)
-constexpr long kStaticMaxTable = 2048;  // complex phase entries per path (digits <= 12 needs 2013)
-constexpr size_t kOffCounter = 0;
-constexpr size_t kOffPartials = 256;
-constexpr size_t kOffProp = kOffPartials + sizeof(double) * 4 * kStaticMaxBlocks;
-constexpr size_t kOffPtab = kOffProp + ((sizeof(Proposal) + 255) / 256) * 256;
-constexpr size_t kOffIdx = kOffPtab + sizeof(double2) * 2 * kStaticMaxTable;
+constexpr int kStaticMaxMoves = 4096;  // candidates per call
+constexpr size_t kOffIdx = 0;
 constexpr size_t kOffDisp = kOffIdx + sizeof(int) * kStaticMaxMoves;
 constexpr size_t kOffDE = kOffDisp + sizeof(double) * 3 * kStaticMaxMoves;
-constexpr size_t kStaticBytes = kOffDE + sizeof(double) * kStaticMaxMoves;
+constexpr size_t kStaticBytes = kOffDE + sizeof(double) * kStaticMaxMoves;  // 144 KB
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 
@@ -2050,15 +2032,7 @@ void DmkTree::shift_batch_static(int m, const long* h_idx, const double* h_disp,
   if (m < 0 || m > kStaticMaxMoves)
     throw std::invalid_argument("static scratch holds at most " + std::to_string(kStaticMaxMoves) +
                                 " candidates per call, got " + std::to_string(m));
-  const long per = 3L * (2 * D.n_window + 1) + long(MAX_LEVELS + 1) * 3 * (2 * D.n_diff + 1);
-  if (per > kStaticMaxTable)
-    throw std::invalid_argument("phase tables of " + std::to_string(per) + " entries exceed the static scratch limit " +
-                                std::to_string(kStaticMaxTable));
   if (m == 0) return;
-  ensure_shift_config();
-  if (shift_grid_ > kStaticMaxBlocks)
-    throw std::invalid_argument("shift grid of " + std::to_string(shift_grid_) +
-                                " blocks exceeds the static scratch limit " + std::to_string(kStaticMaxBlocks));
   unsigned char* base = static_scratch();
   int* s_idx = reinterpret_cast<int*>(base + kOffIdx);
   double* s_disp = reinterpret_cast<double*>(base + kOffDisp);
@@ -2072,34 +2046,15 @@ void DmkTree::shift_batch_static(int m, const long* h_idx, const double* h_disp,
     PDMK_CUDA(cudaMemcpyAsync(s_idx + c0, chunk, sizeof(int) * nc, cudaMemcpyHostToDevice, st_));
   }
   PDMK_CUDA(cudaMemcpyAsync(s_disp, h_disp, sizeof(double) * 3 * m, cudaMemcpyHostToDevice, st_));
-  // the buffer keeps what the last call left; the completion counter must
-  // start at zero, so clear it (a launch that was cut short leaves it set)
-  PDMK_CUDA(cudaMemsetAsync(base + kOffCounter, 0, sizeof(unsigned int), st_));
-  const double pi = 3.14159265358979323846;
-  ShiftArgs a{};
-  a.idx = s_idx;
-  a.disp = s_disp;
-  a.u = nullptr;
-  a.beta = 0.0;
-  a.mode = 0;
-  a.dE_out = s_dE;
-  a.acc_out = nullptr;
-  a.c_window = std::pow(D.delta_k[0], 3) / std::pow(2 * pi, 3);
-  a.partials = reinterpret_cast<double*>(base + kOffPartials);
-  a.counter = reinterpret_cast<unsigned int*>(base + kOffCounter);
-  a.prop = reinterpret_cast<Proposal*>(base + kOffProp);
-  a.ptab = reinterpret_cast<double2*>(base + kOffPtab);
-  a.ptab_per = per;
-  a.cur = nullptr;
   const size_t smem = tables_smem(D, D.max_depth, 2);
-  for (int c = 0; c < m; ++c) {
-    a.move = c;
-    shift_kernel(D.n_poly)<<<unsigned(shift_grid_), SH_T, smem, st_>>>(D, a);
-    PDMK_LAUNCH_CHECK();
-  }
+  const ShiftBatchKernel kern = shift_batch_kernel(D.n_poly);
+  raise_smem_limit(reinterpret_cast<const void*>(kern), smem);
+  const double pi = 3.14159265358979323846;
+  const double c_window = std::pow(D.delta_k[0], 3) / std::pow(2 * pi, 3);
+  kern<<<unsigned(m), SB_T, smem, st_>>>(D, s_idx, s_disp, c_window, s_dE);
+  PDMK_LAUNCH_CHECK();
   PDMK_CUDA(cudaMemcpyAsync(h_dE, s_dE, sizeof(double) * m, cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaStreamSynchronize(st_));
-  last_valid_ = false;
 }
 
 // Metropolis sequences of many trees in one launch (k_mc_rep), ordered after
@@ -2127,8 +2082,7 @@ void DmkTree::replicas_mc_run(const std::vector<DmkTree*>& ts, int m, const int*
   PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_trees), sizeof(DevTree) * hd.size(), st));
   PDMK_CUDA(cudaMemcpyAsync(d_trees, hd.data(), sizeof(DevTree) * hd.size(), cudaMemcpyHostToDevice, st));
   const McRepKernel kern = mc_rep_kernel(np);
-  static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function
-  raise_smem_limit(reinterpret_cast<const void*>(kern), smem, smem_set[(np - 7) / 6]);
+  raise_smem_limit(reinterpret_cast<const void*>(kern), smem);
   kern<<<unsigned(ts.size()), REP_T, smem, st>>>(d_trees, m, d_idx, d_disp, d_u, beta, d_dE, d_acc);
   PDMK_LAUNCH_CHECK();
   PDMK_CUDA(cudaFreeAsync(d_trees, st));
@@ -2150,8 +2104,7 @@ void DmkTree::potential_batch(int m, const int* d_idx, double* d_phi, double* d_
   prepare_box_lists();  // the per-level self terms S_l
   const size_t smem = tables_smem(D, D.max_depth, 1);
   const PotentialKernel kern = potential_kernel(D.n_poly);
-  static size_t smem_set[4] = {0, 0, 0, 0};  // the attribute is per function, shared by all trees
-  raise_smem_limit(reinterpret_cast<const void*>(kern), smem, smem_set[(D.n_poly - 7) / 6]);
+  raise_smem_limit(reinterpret_cast<const void*>(kern), smem);
   const double pi = 3.14159265358979323846;
   const double c_window = std::pow(D.delta_k[0], 3) / std::pow(2 * pi, 3);
   const double self_w = ps_.psi0_0 / (2 * D.boxsize[2] * ps_.C0);

@@ -185,6 +185,7 @@ struct EnergyParts {
 struct TreeOptions {
   int leaf_slack = 0;      // extra particle slots per leaf for moves
   int pool_capacity = 4096;
+  int precision = 0;       // 0: FP64 outgoing pass; 1: int8-sliced tensor-core outgoing pass (mixed)
 };
 
 class DmkTree {
@@ -343,6 +344,15 @@ class DmkTree {
   void build_mc_graph(int timed);
   void launch_shift_cursor(int move);
   cudaStream_t aux_ = nullptr;  // second stream for the root plane-wave pass
+  // mixed precision: [0] max |q| (fixed-point scale), [1] error word (as int) of the tensor-core pass
+  double* d_mix_ = nullptr;
+  bool qmax_ready_ = false;
+ public:
+  int precision() const { return opt_.precision; }
+  // error word of the mixed pass (nonzero: a pipeline wait gave up); synchronises
+  int check_mixed_error();
+
+ private:
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   double2* ptab_ = nullptr;  // phase tables of the last proposal, both paths
   long ptab_per_ = 0;

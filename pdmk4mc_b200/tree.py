@@ -23,6 +23,8 @@ PROXY = 2
 STATIC_MAX_MOVES = 4096  # HPDMK_STATIC_MAX_MOVES in include/hpdmk.h
 MC_PERSISTENT = 0  # HPDMK_MC_PERSISTENT
 MC_GRAPH = 1  # HPDMK_MC_GRAPH
+PRECISION_FP64 = 0  # HPDMK_PRECISION_FP64
+PRECISION_MIXED = 1  # HPDMK_PRECISION_MIXED: outgoing expansions on the tensor cores from int8 slices
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -212,13 +214,14 @@ class HPDMKPtTree:
     """Device-resident DMK tree (reference: HPDMKPtTree<double>, include/tree.hpp:29-132)."""
 
     def __init__(self, params: HPDMKParams, r_src, charge, leaf_slack: int = 8, pool_capacity: int = 4096,
-                 device: int = 0, stream=None, device_inputs=None):
-        """r_src / charge: host arrays; or, with device_inputs=(d_r_ptr, d_q_ptr, n), device pointers."""
+                 device: int = 0, stream=None, device_inputs=None, precision: int = PRECISION_FP64):
+        """r_src / charge: host arrays; or, with device_inputs=(d_r_ptr, d_q_ptr, n), device pointers.
+        precision: PRECISION_FP64 (default) or PRECISION_MIXED."""
         L = load_library()
         self.params = params
         cp = _Params(int(params.n_per_leaf), int(params.digits), float(params.L), float(params.prolate_order),
                      int(params.init))
-        ext = _ExtParams(int(leaf_slack), int(pool_capacity), 0, int(device), stream)
+        ext = _ExtParams(int(leaf_slack), int(pool_capacity), int(precision), int(device), stream)
         if device_inputs is not None:
             d_r, d_q, n = device_inputs
             self._h = L.hpdmk_tree_init_device(0, cp, ctypes.byref(ext), int(n), d_r, d_q)

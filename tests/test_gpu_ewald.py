@@ -81,17 +81,36 @@ def test_dmk_vs_gpu_ewald_digits(digits):
         t.close()
 
 
-def test_dmk_vs_gpu_ewald_n1e6():
+def clustered(n, L, seed, n_clusters=64, frac=0.8):
+    """64 isotropic Gaussian clusters (centres uniform, sigma = L/40) plus a 20 % uniform background."""
+    rng = np.random.default_rng(seed)
+    m = int(frac * n)
+    c = rng.uniform(0, L, (n_clusters, 3))
+    r = np.concatenate([np.mod(c[rng.integers(0, n_clusters, m)] + rng.normal(0, L / 40, (m, 3)), L),
+                        rng.uniform(0, L, (n - m, 3))])
+    r[r >= L] = 0.0  # a wrap that rounds to L
+    return np.ascontiguousarray(r.reshape(-1))
+
+
+# The target accuracy at N = 1e6: 1e-8 relative to the FP64 Ewald energy, for
+# the FP64 path and the mixed-precision path, on the uniform cube (the
+# candidate-query configuration) and the clustered system.
+@pytest.mark.parametrize("kind", ["uniform", "clustered"])
+@pytest.mark.parametrize("precision", [P.PRECISION_FP64, P.PRECISION_MIXED])
+def test_dmk_vs_gpu_ewald_n1e6(kind, precision):
     n, L = 1_000_000, 100.0
     rng = np.random.default_rng(21)
-    r = rng.uniform(0, L, 3 * n)
+    r = rng.uniform(0, L, 3 * n) if kind == "uniform" else clustered(n, L, 21)
     q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
-    t = P.HPDMKPtTree(P.HPDMKParams(n_per_leaf=200, digits=9, L=L, init=P.DIRECT), r, q, leaf_slack=0)
+    t = P.HPDMKPtTree(P.HPDMKParams(n_per_leaf=200, digits=9, L=L, init=P.DIRECT), r, q, leaf_slack=0,
+                      precision=precision)
     try:
         e, _ = t.ewald_energy()
         t.form_outgoing_pw()
         t.form_incoming_pw()
         dmk = t.eval_energy()
-        assert abs(dmk - e) <= 5e-8 * abs(e), (dmk, e)
+        rel = abs(dmk - e) / abs(e)
+        print(f"\nACCURACY n1e6 {kind} precision={precision} depth={t.max_depth} dmk={dmk!r} ewald={e!r} rel={rel:.3e}")
+        assert rel <= 1e-8, (dmk, e, rel)
     finally:
         t.close()

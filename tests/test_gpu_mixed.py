@@ -1,0 +1,157 @@
+"""Mixed precision (HPDMK_PRECISION_MIXED): the outgoing plane-wave
+expansions formed on the tensor cores (tcgen05 kind::i8) from three 7-bit
+slices of each phase factor, against the oracle's FP64 expansions (the
+reference's nudft3d1_halfplane, include/nudft.hpp:95-121, and the root pass,
+src/planewave.cpp:24-46); the energies and energy shifts that follow from
+them against the oracle and the FP64 Ewald energy."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import pdmk4mc_b200 as P
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# Each slice product is exact (32-bit integer sums); the operands carry a
+# truncation error of at most 2^-21 of their range (|factor| <= 1, charges
+# scaled by max |q|). A coefficient of a box of n particles is off by at most
+# n 2^-20 max|q|, and for the random phases of a box near sqrt(n) 3e-7: the
+# bound below is relative to the largest coefficient of the box.
+REL_PW_MIXED = 5e-6
+# energies: the mixed energy against the FP64 one, relative to |E| (the
+# accuracy target of the mixed path is 1e-8 against Ewald)
+REL_E_MIXED = 1e-8
+ABS_DE_MIXED = 1e-8
+
+
+def system(kind, n, L, seed=0):
+    rng = np.random.default_rng(seed)
+    if kind == "uniform":
+        r = rng.uniform(0, L, (n, 3))
+    elif kind == "clustered":
+        c = rng.uniform(0, L, (6, 3))
+        m = int(0.8 * n)
+        r = np.concatenate([np.mod(c[rng.integers(0, 6, m)] + rng.normal(0, L / 40, (m, 3)), L),
+                            rng.uniform(0, L, (n - m, 3))])
+    elif kind == "reference":
+        return O.reference_test_system(n, L)
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    return np.ascontiguousarray(r.reshape(-1)), q
+
+
+CASES = [
+    # (kind, n, L, n_per_leaf, digits): every supported digits setting, so
+    # every mode count of the mixed kernel (window and difference) runs
+    ("uniform", 1000, 10.0, 10, 6),      # the reference's first configuration
+    ("reference", 1000, 20.0, 10, 3),
+    ("clustered", 6000, 20.0, 20, 9),
+    ("uniform", 3000, 46.4, 8, 12),
+]
+
+
+def mixed_tree(r, q, L, npl, digits, slack=8):
+    return P.HPDMKPtTree(P.HPDMKParams(n_per_leaf=npl, digits=digits, L=L, init=P.DIRECT), r, q,
+                         leaf_slack=slack, precision=P.PRECISION_MIXED)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_mixed_expansions_and_energy(case):
+    kind, n, L, npl, digits = case
+    r, q = system(kind, n, L)
+    g = mixed_tree(r, q, L, npl, digits)
+    o = O.OracleTree(L, npl, digits, r, q)
+    try:
+        for t in (g, o):
+            t.form_outgoing_pw()
+            t.form_incoming_pw()
+        ro, rg = o.pw(0), g.pw(0)
+        assert np.abs(rg - ro).max() <= REL_PW_MIXED * np.abs(ro).max(), np.abs(rg - ro).max() / np.abs(ro).max()
+        lv, pf, leaf, cnt = o.tree_nodes()
+        worst = 0.0
+        for node in np.nonzero((lv >= 2) & (lv <= o.max_depth - 2))[0][:300]:
+            a, b = g.pw(node), o.pw(node)
+            scale = max(np.abs(b).max(), 1e-300)
+            worst = max(worst, np.abs(a - b).max() / scale)
+        assert worst <= REL_PW_MIXED, worst
+        pg, po = g.eval_energy_parts(), o.eval_energy_parts()
+        E = po.sum()
+        assert abs(pg.sum() - E) <= REL_E_MIXED * abs(E), (pg, po, abs(pg.sum() - E) / abs(E))
+        # the near field does not depend on the expansions: unchanged
+        assert abs(pg[2] - po[2]) <= 1e-11 * abs(E)
+    finally:
+        g.close()
+
+
+def test_mixed_shifts_updates_and_metropolis():
+    # energy shifts read the incoming expansions that the mixed pass formed;
+    # the shift itself and the update stay FP64
+    r, q = system("clustered", 6000, 20.0, seed=2)
+    g = mixed_tree(r, q, 20.0, 20, 9)
+    o = O.OracleTree(20.0, 20, 9, r, q)
+    try:
+        for t in (g, o):
+            t.form_outgoing_pw()
+            t.form_incoming_pw()
+        rng = np.random.default_rng(3)
+        for step in range(16):
+            i = int(rng.integers(0, 6000))
+            d = rng.uniform(-0.5, 0.5, 3)
+            dg = g.eval_shift_energy(i, *d)
+            do = o.eval_shift_energy(i, *d)
+            assert abs(dg - do) <= ABS_DE_MIXED * max(1.0, abs(do)), (step, dg, do)
+            if step % 2 == 0:
+                g.update_shift(i, *d)
+                o.update_shift(i, *d)
+        m = 200
+        idx = rng.integers(0, 6000, m)
+        disp = rng.uniform(-0.3, 0.3, (m, 3))
+        u = rng.uniform(0, 1, m)
+        dEm, acc = g.mc_run(idx, disp, u, 1.0)
+        for c in range(m):
+            de = o.eval_shift_energy(int(idx[c]), *disp[c])
+            assert abs(dEm[c] - de) <= ABS_DE_MIXED * max(1.0, abs(de)), (c, dEm[c], de)
+            # the same decision (no move sits within 1e-8 of the threshold here)
+            assert bool(acc[c]) == bool(u[c] < np.exp(-de)), c
+            if acc[c]:
+                o.update_shift(int(idx[c]), *disp[c])
+        np.testing.assert_array_equal(g.positions(), o.positions())
+        # a new outgoing pass on the moved particles
+        g.form_outgoing_pw()
+        g.form_incoming_pw()
+        o.form_outgoing_pw()
+        o.form_incoming_pw()
+        E, Eo = g.eval_energy(), o.eval_energy()
+        assert abs(E - Eo) <= REL_E_MIXED * abs(Eo), (E, Eo)
+    finally:
+        g.close()
+
+
+def test_mixed_bench_workload_vs_ewald():
+    # uniform N = 1e5, L = 46.4, 9 digits: the mixed energy against the stored
+    # FP64 Ewald energy of the same positions, at the 1e-8 target
+    import sys
+    sys.path.insert(0, os.path.dirname(HERE))
+    import bench
+    gl = json.load(open(os.path.join(HERE, "golden", "bench_ewald.json")))
+    W = bench.WORKLOAD_N1E5
+    r, q = bench.make_system(1, W["N"], W["L"])
+    assert gl["workload"]["N"] == W["N"] and gl["workload"]["L"] == W["L"] and gl["workload"]["seed"] == 1
+    params = P.HPDMKParams(n_per_leaf=W["n_per_leaf"], digits=W["digits"], L=W["L"], init=P.DIRECT)
+    g = P.HPDMKPtTree(params, r, q, precision=P.PRECISION_MIXED)
+    f = P.HPDMKPtTree(params, r, q)
+    try:
+        for t in (g, f):
+            t.form_outgoing_pw()
+            t.form_incoming_pw()
+        Em, Ef = g.eval_energy(), f.eval_energy()
+        ew = gl["ewald"]["energy"]
+        assert abs(Em - ew) <= 1e-8 * abs(ew), (Em, ew, abs(Em - ew) / abs(ew))
+        assert abs(Em - Ef) <= 1e-8 * abs(Ef), (Em, Ef)
+    finally:
+        g.close()
+        f.close()

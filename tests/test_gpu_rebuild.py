@@ -2,11 +2,16 @@
 and arrivals overflow into the pool), hpdmk_tree_rebuild re-bins the tree on
 the device. The rebuilt tree must equal a tree built from the current
 positions: the same nodes, neighbour lists and particle order, the same
-energies and energy shifts, and the same Metropolis run afterwards."""
+energies and energy shifts, and the same Metropolis run afterwards; and it
+must match the oracle's tree built from those positions (nodes, neighbour
+lists and order bit for bit, energy parts to the parity tolerance)."""
 import numpy as np
 import pytest
 
 import pdmk4mc_b200 as P
+from oracle import oracle as O
+
+REL_E = 1e-11
 
 pytestmark = pytest.mark.gpu
 
@@ -37,7 +42,18 @@ def test_rebuild_equals_fresh_tree(mode):
     f.set_mc_mode(mode)
     f.form_outgoing_pw()
     f.form_incoming_pw()
+    o = O.OracleTree(L, npl, digits, pos, q)
+    o.form_outgoing_pw()
+    o.form_incoming_pw()
     try:
+        assert (t.max_depth, t.n_nodes) == (o.max_depth, o.n_nodes)
+        for a, b in zip(t.tree_nodes(), o.tree_nodes()):
+            np.testing.assert_array_equal(a, b)
+        for a, b in zip(t.tree_neighbors(), o.tree_neighbors()):
+            np.testing.assert_array_equal(a, b)
+        np.testing.assert_array_equal(t.sorted_order(), o.sorted_order())
+        pt, po = t.eval_energy_parts(), o.eval_energy_parts()
+        assert np.all(np.abs(pt - po) <= REL_E * abs(po.sum())), (pt, po)
         assert (t.max_depth, t.n_nodes) == (f.max_depth, f.n_nodes)
         for a, b in zip(t.tree_nodes(), f.tree_nodes()):
             np.testing.assert_array_equal(a, b)

@@ -1,11 +1,13 @@
 """Replica sets: many independent trees of uneven size run their Metropolis
 sequences in one launch (one block per tree). Each replica must reproduce its
 own single-tree run: the same accept decisions and final positions, energy
-shifts within the parity tolerance, and maintained energies that match."""
+shifts within the parity tolerance, and maintained energies that match; two
+replicas are also replayed move by move on the oracle's tree."""
 import numpy as np
 import pytest
 
 import pdmk4mc_b200 as P
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -24,7 +26,7 @@ def test_replicas_match_single_tree_runs(digits):
     sizes = [2000, 3500, 6000, 9000, 15000, 24000]
     m = 64
     rng = np.random.default_rng(100 + digits)
-    reps, twins, moves = [], [], []
+    reps, twins, moves, oracles = [], [], [], []
     for k, n in enumerate(sizes):
         r, q, L = system(n, k)
         npl = max(16, n // 128)  # depth >= 3 for every replica
@@ -36,12 +38,25 @@ def test_replicas_match_single_tree_runs(digits):
             t.form_incoming_pw()
         reps.append(a)
         twins.append(b)
+        if k < 2:
+            o = O.OracleTree(L, npl, digits, r, q)
+            o.form_outgoing_pw()
+            o.form_incoming_pw()
+            oracles.append(o)
         moves.append((rng.integers(0, n, m), rng.uniform(-0.3, 0.3, (m, 3)), rng.uniform(0, 1, m)))
     try:
         idx = np.stack([mv[0] for mv in moves])
         disp = np.stack([mv[1] for mv in moves])
         u = np.stack([mv[2] for mv in moves])
         dE, acc = P.replicas_mc_run(reps, idx, disp, u, 1.0)
+        for k, o in enumerate(oracles):
+            for c in range(m):
+                de = o.eval_shift_energy(int(idx[k, c]), *disp[k, c])
+                assert abs(dE[k, c] - de) <= ABS_DE * max(1.0, abs(de)), (k, c, dE[k, c], de)
+                assert bool(acc[k, c]) == bool(u[k, c] < np.exp(-de)), (k, c)
+                if acc[k, c]:
+                    o.update_shift(int(idx[k, c]), *disp[k, c])
+            np.testing.assert_array_equal(reps[k].positions(), o.positions())
         for k in range(len(sizes)):
             d1, a1 = twins[k].mc_run(moves[k][0], moves[k][1], moves[k][2], 1.0)
             np.testing.assert_array_less(np.abs(dE[k] - d1), ABS_DE * np.maximum(1.0, np.abs(d1)))
