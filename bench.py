@@ -1,16 +1,26 @@
 """Benchmark: MC trial moves/s and full-energy evaluations/s of the periodic DMK
-energy path on one B200 (FP64 path, 1e-8 accuracy setting: 9 digits).
+energy path on one B200, mixed precision against FP64, at 9 digits (the
+1e-8 accuracy setting), each result with its error against an FP64 Ewald.
 
-Workload (one GPU): N = 1e5 point charges, uniform in a periodic cube of
-side L = 46.4 (density ~1), alternating +1/-1 charges (net neutral), 9-digit
-DMK (PSWF tolerance 1e-9), n_per_leaf = 200. One step = one full energy
-evaluation from raw positions resident in HBM (tree build, outgoing and
-incoming plane waves, window + difference + residual energies) followed by
-10^4 sequential Metropolis moves (displacement uniform in [-0.3, 0.3]^3,
-beta = 1) with accept-and-update. Inputs are seeded synthetic data; no
-dataset is involved.
+Headline workload (one GPU): N = 1e6 point charges uniform in a periodic cube
+of side L = 100, alternating +1/-1 charges (net neutral), 9-digit DMK,
+n_per_leaf = 200 (tree depth 6). Each step, for the FP64 path and for the
+mixed-precision path (outgoing expansions on the tensor cores from int8
+slices), from inputs resident in HBM:
+  - one full energy from raw positions (tree build, outgoing and incoming
+    plane waves, window + difference + residual energies);
+  - 10^4 sequential Metropolis moves (displacement uniform in [-0.3, 0.3]^3,
+    beta = 1) with accept-and-update, one persistent launch;
+  - 4096 candidate moves (displacement uniform in [-0.5, 0.5]^3) evaluated as
+    energy shifts against one state in one launch.
+`value` is the mixed path's Metropolis trial moves/s; the line also carries
+both paths' numbers and their ratios, the clustered system (64 Gaussian
+clusters, sigma = L/40, plus 20 % uniform background, N = 1e6, L = 100) and
+the N = 1e5, L = 46.4 cube. Inputs are seeded synthetic data; no dataset is
+involved.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py --profile n1e5|n1e6 [--precision mixed|fp64]   (short run for profilers)
 
 With --gpus N > 1 (torchrun) every rank runs an independent replica of the
 workload (the method does not shard: replicas only) and the whole-job value
@@ -23,6 +33,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -31,9 +42,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "MC trial moves/s & full-energy evals/s, mixed vs FP64 GPU at 1e-8 rel err"
-WORKLOAD = dict(workload="uniform periodic cube, Metropolis MC + full energy", N=100000, L=46.4, digits=9,
-                n_per_leaf=200, moves_per_step=10000, step=0.3, beta=1.0, charges="alternating +1/-1")
-WORKLOAD_N1E5 = WORKLOAD
+WORKLOAD = dict(workload="uniform periodic cube, full energy + sequential Metropolis + 4096-candidate batch, "
+                         "mixed precision and FP64", N=1_000_000, L=100.0, digits=9, n_per_leaf=200,
+                moves_per_step=10000, candidates=4096, step=0.3, candidate_step=0.5, beta=1.0,
+                charges="alternating +1/-1")
+CLUSTERED = dict(workload="64 isotropic Gaussian clusters (sigma = L/40) + 20 % uniform background", N=1_000_000,
+                 L=100.0, digits=9, n_per_leaf=200, moves_per_step=2000, step=0.3, beta=1.0,
+                 charges="alternating +1/-1")
+WORKLOAD_N1E5 = dict(workload="uniform periodic cube, full energy + sequential Metropolis", N=100000, L=46.4,
+                     digits=9, n_per_leaf=200, moves_per_step=10000, step=0.3, beta=1.0,
+                     charges="alternating +1/-1")
 
 
 def make_system(seed, n, L):
@@ -41,6 +59,16 @@ def make_system(seed, n, L):
     r = rng.uniform(0.0, L, 3 * n)
     q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
     return r, q
+
+
+def make_clustered(seed, n, L, n_clusters=64, frac=0.8):
+    rng = np.random.default_rng(seed)
+    m = int(frac * n)
+    c = rng.uniform(0, L, (n_clusters, 3))
+    r = np.concatenate([np.mod(c[rng.integers(0, n_clusters, m)] + rng.normal(0, L / 40, (m, 3)), L),
+                        rng.uniform(0, L, (n - m, 3))])
+    r[r >= L] = 0.0  # a wrap that rounds to L
+    return np.ascontiguousarray(r.reshape(-1)), np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
 
 
 def make_moves(seed, n, m, step):
@@ -141,8 +169,11 @@ def barrier(ws):
         dist.barrier()
 
 
-def cpu_baseline_sample(W):
-    """The oracle port (CPU restatement of the reference algorithm) on a bounded sample."""
+def cpu_baseline_sample(W, moves=40):
+    """The oracle port (CPU restatement of the reference algorithm) on a
+    bounded sample of the workload: one full energy on all host threads and
+    `moves` sequential Metropolis moves on one thread (the reference times its
+    moves on one thread, benchmark/dmk_energyshift_runtime.cpp:43-44)."""
     from oracle import oracle as O
     n, L = W["N"], W["L"]
     r, q = make_system(7, n, L)
@@ -155,45 +186,200 @@ def cpu_baseline_sample(W):
     T.form_incoming_pw()
     E = T.eval_energy()
     t_energy = time.perf_counter() - t0
-    m = 40
-    idx, disp, u = make_moves(7, n, m, W["step"])
+    idx, disp, u = make_moves(7, n, moves, W["step"])
     T.nthreads = 1
     t0 = time.perf_counter()
     acc = 0
-    for c in range(m):
+    for c in range(moves):
         dE = T.eval_shift_energy(idx[c], *disp[c])
         if u[c] < np.exp(-W["beta"] * dE):
             T.update_shift(idx[c], *disp[c])
             acc += 1
     t_moves = time.perf_counter() - t0
-    return dict(moves_per_s=m / t_moves, energy_evals_per_s=1.0 / t_energy, t_build_s=t_build, energy=E,
-                cores=ncores, moves=m, accepted=acc)
+    return dict(moves_per_s=moves / t_moves, energy_evals_per_s=1.0 / t_energy, t_build_s=t_build, energy=E,
+                cores=ncores, moves=moves, accepted=acc)
 
 
 def run_reference(args, rank, ws):
+    """The reference's algorithm on the host cores (the oracle port: the
+    reference's C++ path cannot be built here). The oracle tree is built and
+    its full energy timed once; each step is a sample of 20 sequential
+    Metropolis moves on one thread, and ms_per_step is that sample's time."""
     if rank != 0:
         return
+    from oracle import oracle as O
     W = dict(WORKLOAD)
-    vals = []
-    ee = []
+    n, L = W["N"], W["L"]
+    r, q = make_system(7, n, L)
+    ncores = os.cpu_count() or 1
+    T = O.OracleTree(L, W["n_per_leaf"], W["digits"], r, q, nthreads=ncores)
+    t0 = time.perf_counter()
+    T.form_outgoing_pw()
+    T.form_incoming_pw()
+    T.eval_energy()
+    t_energy = time.perf_counter() - t0
+    T.nthreads = 1
+    per = 20
+    idx, disp, u = make_moves(7, n, per * (args.warmup + args.steps), W["step"])
+    times = []
     for s in range(args.warmup + args.steps):
-        res = cpu_baseline_sample(W)
+        t0 = time.perf_counter()
+        for c in range(s * per, (s + 1) * per):
+            dE = T.eval_shift_energy(idx[c], *disp[c])
+            if u[c] < np.exp(-W["beta"] * dE):
+                T.update_shift(idx[c], *disp[c])
         if s >= args.warmup:
-            vals.append(res["moves_per_s"])
-            ee.append(res["energy_evals_per_s"])
-    v = float(np.mean(vals))
+            times.append(time.perf_counter() - t0)
+    v = per * len(times) / float(np.sum(times))
+    cfg = dict(W, moves_per_step=per, parallelism="replicas" if ws > 1 else "single")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "moves/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * W["moves_per_step"] / v,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(W, parallelism="replicas" if ws > 1 else "single"),
-        "full_energy_evals_per_s": float(np.mean(ee)),
+        "config": cfg,
+        "full_energy_evals_per_s": 1.0 / t_energy,
         "cpu_baseline": {"value": v, "unit": "moves/s", "cores": 1, "kind": "port",
-                         "sample": f"{res['moves']} sequential Metropolis moves (1 thread, as the reference's "
-                                   f"timing driver) + 1 full energy on {res['cores']} threads, per step"},
+                         "sample": f"{per} sequential Metropolis moves per step on 1 thread (as the reference's "
+                                   f"timing driver) on the N = 1e6 cube; full energy timed once on {ncores} "
+                                   f"threads"},
         "e2e": {"value": v, "unit": "moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+class Arm:
+    """One precision on one system: the Metropolis tree (with slack for moves)
+    and the device-resident inputs of every step."""
+
+    def __init__(self, P, torch, W, r, q, precision, n_moves_total, seed, cand=0):
+        self.P, self.torch, self.W = P, torch, W
+        self.precision = precision
+        n, L = W["N"], W["L"]
+        self.params = P.HPDMKParams(n_per_leaf=W["n_per_leaf"], digits=W["digits"], L=L, init=P.DIRECT)
+        self.d_r = torch.tensor(r, dtype=torch.float64, device="cuda")
+        self.d_q = torch.tensor(q, dtype=torch.float64, device="cuda")
+        idx, disp, u = make_moves(seed, n, max(n_moves_total, 1), W["step"])
+        self.d_idx = torch.tensor(idx, dtype=torch.int32, device="cuda")
+        self.d_disp = torch.tensor(disp.reshape(-1), dtype=torch.float64, device="cuda")
+        self.d_u = torch.tensor(u, dtype=torch.float64, device="cuda")
+        M = W["moves_per_step"]
+        self.d_dE = torch.zeros(M, dtype=torch.float64, device="cuda")
+        self.d_acc = torch.zeros(M, dtype=torch.int32, device="cuda")
+        self.cand = cand
+        if cand:
+            ci, cd, _ = make_moves(seed + 77, n, cand, W.get("candidate_step", 0.5))
+            self.c_idx = torch.tensor(ci, dtype=torch.int32, device="cuda")
+            self.c_disp = torch.tensor(cd.reshape(-1), dtype=torch.float64, device="cuda")
+            self.c_dE = torch.zeros(cand, dtype=torch.float64, device="cuda")
+        self.tree = P.HPDMKPtTree(self.params, r, q, leaf_slack=8, precision=precision)
+        self.stream = torch.cuda.ExternalStream(self.tree.stream_ptr())
+        self.estream = torch.cuda.Stream()
+        self.tree.form_outgoing_pw()
+        self.tree.form_incoming_pw()
+        self.tree.eval_energy()
+        self.t_energy, self.t_moves, self.t_cand = [], [], []
+        self.work = np.zeros(3)
+        self.energy = None
+
+    def full_energy(self, timed):
+        """Tree build + outgoing + incoming + energy from HBM-resident positions."""
+        P, torch = self.P, self.torch
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(self.estream)
+        ef = P.HPDMKPtTree(self.params, None, None, leaf_slack=0, stream=self.estream.cuda_stream,
+                           device_inputs=(self.d_r.data_ptr(), self.d_q.data_ptr(), self.W["N"]),
+                           precision=self.precision)
+        ef.form_outgoing_pw()
+        ef.form_incoming_pw()
+        self.energy = ef.eval_energy()
+        e1.record(self.estream)
+        torch.cuda.synchronize()
+        ef.close()
+        if timed:
+            self.t_energy.append(e0.elapsed_time(e1) / 1e3)
+
+    def moves(self, step_index, timed):
+        torch = self.torch
+        M = self.W["moves_per_step"]
+        off = step_index * M
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        self.tree.mc_run_device(M, self.d_idx[off:].data_ptr(), self.d_disp[3 * off:].data_ptr(),
+                                self.d_u[off:].data_ptr(), self.W["beta"], self.d_dE.data_ptr(),
+                                self.d_acc.data_ptr())
+        e1.record(self.stream)
+        torch.cuda.synchronize()
+        if timed:
+            self.t_moves.append(e0.elapsed_time(e1) / 1e3)
+            self.work += self.tree.update_work()
+
+    def candidates(self, timed):
+        if not self.cand:
+            return
+        torch = self.torch
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        self.tree.eval_shift_energy_batch_device(self.cand, self.c_idx.data_ptr(), self.c_disp.data_ptr(),
+                                                 self.c_dE.data_ptr())
+        e1.record(self.stream)
+        torch.cuda.synchronize()
+        if timed:
+            self.t_cand.append(e0.elapsed_time(e1) / 1e3)
+
+    def summary(self, ws, ewald):
+        M = self.W["moves_per_step"]
+        tm = all_max(float(np.sum(self.t_moves)), ws)
+        te = all_max(float(np.sum(self.t_energy)), ws)
+        out = {"moves_per_s": ws * M * len(self.t_moves) / tm,
+               "full_energy_evals_per_s": ws * len(self.t_energy) / te,
+               "full_energy_ms": 1e3 * te / len(self.t_energy),
+               "accept_rate": self.work[0] / (M * len(self.t_moves)),
+               "energy": self.energy}
+        if self.t_cand:
+            tc = all_max(float(np.sum(self.t_cand)), ws)
+            out["candidates_per_s"] = ws * self.cand * len(self.t_cand) / tc
+            out["candidate_batch_ms"] = 1e3 * tc / len(self.t_cand)
+        if ewald is not None:
+            out["rel_err_vs_ewald"] = abs(self.energy - ewald) / abs(ewald)
+        return out
+
+    def close(self):
+        self.tree.close()
+
+
+def run_system(P, torch, W, r, q, args, ws, l2_flush, seed, cand, with_timing=False):
+    """FP64 and mixed arms on one system, alternating step by step; returns
+    (arms, launches in the timed region)."""
+    M = W["moves_per_step"]
+    nsteps = args.warmup + args.steps
+    arms = {"fp64": Arm(P, torch, W, r, q, P.PRECISION_FP64, M * nsteps, seed, cand),
+            "mixed": Arm(P, torch, W, r, q, P.PRECISION_MIXED, M * nsteps, seed, cand)}
+    launches = 0
+    for s in range(nsteps):
+        timed = s >= args.warmup
+        if with_timing and s == args.warmup:
+            arms["mixed"].tree.get_timing(reset=True)
+            arms["mixed"].tree.set_timing(True)
+        for name in ("fp64", "mixed"):
+            a = arms[name]
+            barrier(ws)
+            l0 = P.launch_count()
+            l2_flush.zero_()
+            torch.cuda.synchronize()
+            a.full_energy(timed)
+            l2_flush.zero_()
+            torch.cuda.synchronize()
+            a.moves(s, timed)
+            l2_flush.zero_()
+            torch.cuda.synchronize()
+            a.candidates(timed)
+            barrier(ws)
+            if timed:
+                launches += P.launch_count() - l0
+    return arms, launches
 
 
 def run_b200(args, rank, ws):
@@ -204,155 +390,190 @@ def run_b200(args, rank, ws):
     torch.cuda.set_device(dev)
     W = dict(WORKLOAD)
     W["moves_per_step"] = args.moves_per_step
-    n, L, M = W["N"], W["L"], W["moves_per_step"]
-    params = P.HPDMKParams(n_per_leaf=W["n_per_leaf"], digits=W["digits"], L=L, init=P.DIRECT)
-    r, q = make_system(1 + rank, n, L)
-    # inputs resident in HBM for the device-timed value
-    idx, disp, u = make_moves(1 + rank, n, M * (args.steps + args.warmup), W["step"])
-    d_idx = torch.tensor(idx, dtype=torch.int32, device="cuda")
-    d_disp = torch.tensor(disp.reshape(-1), dtype=torch.float64, device="cuda")
-    d_u = torch.tensor(u, dtype=torch.float64, device="cuda")
-    d_dE = torch.zeros(M, dtype=torch.float64, device="cuda")
-    d_acc = torch.zeros(M, dtype=torch.int32, device="cuda")
-    d_r = torch.tensor(r, dtype=torch.float64, device="cuda")
-    d_q = torch.tensor(q, dtype=torch.float64, device="cuda")
-    # MC tree (slack for moves); its stream carries every kernel
-    tree = P.HPDMKPtTree(params, r, q, leaf_slack=8)
-    tree.set_mc_mode(P.MC_GRAPH if args.mc_mode == "graph" else P.MC_PERSISTENT)
-    stream = torch.cuda.ExternalStream(tree.stream_ptr())
-    tree.form_outgoing_pw()
-    tree.form_incoming_pw()
-    tree.eval_energy()
-    estream = torch.cuda.Stream()
-
-    t_moves = []
-    t_energy = []
-    work = np.zeros(3)
-    launches = 0
+    n, L = W["N"], W["L"]
     l2_flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    clk_path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv") if os.path.isdir(
-        os.path.join(ROOT, "gpurun_out")) else "/tmp/pdmk_clocks.csv"
-    with Clocks(clk_path) as clk:
-        for s in range(args.warmup + args.steps):
-            timed = s >= args.warmup
-            if timed and s == args.warmup:
-                tree.get_timing(reset=True)
-                tree.set_timing(True)
-            barrier(ws)
-            l2_flush.zero_()
-            torch.cuda.synchronize()
-            # energy phase: tree build + outgoing + incoming + energy from HBM-resident inputs
-            ee0 = torch.cuda.Event(enable_timing=True)
-            ee1 = torch.cuda.Event(enable_timing=True)
-            ee0.record(estream)
-            if timed:
-                launches0 = P.launch_count()
-            ef = P.HPDMKPtTree(params, None, None, leaf_slack=0, stream=estream.cuda_stream,
-                               device_inputs=(d_r.data_ptr(), d_q.data_ptr(), n))
-            ef.form_outgoing_pw()
-            ef.form_incoming_pw()
-            e_dmk = ef.eval_energy()
-            ee1.record(estream)
-            torch.cuda.synchronize()
-            ef.close()
-            # move phase, device-resident proposals
-            ev0 = torch.cuda.Event(enable_timing=True)
-            ev1 = torch.cuda.Event(enable_timing=True)
-            off = s * M
-            ev0.record(stream)
-            tree.mc_run_device(M, d_idx[off:].data_ptr(), d_disp[3 * off:].data_ptr(), d_u[off:].data_ptr(),
-                               W["beta"], d_dE.data_ptr(), d_acc.data_ptr())
-            ev1.record(stream)
-            torch.cuda.synchronize()
-            barrier(ws)
-            if timed:
-                launches += P.launch_count() - launches0
-                t_moves.append(ev0.elapsed_time(ev1) / 1e3)
-                t_energy.append(ee0.elapsed_time(ee1) / 1e3)
-                work += tree.update_work()
-        timing = tree.get_timing()
-        tree.set_timing(False)
-    tm = all_max(float(np.sum(t_moves)), ws)
-    te = all_max(float(np.sum(t_energy)), ws)
-    moves_per_s = ws * M * args.steps / tm
-    energy_per_s = ws * args.steps / te
-    # roofline of the dominant MC kernel, HBM bound. Persistent mode: k_mc,
-    # one launch per step, bytes = dE reads + update read-modify-writes of all
-    # timed moves. Graph mode: k_update, bytes over every timed move, duration
-    # from the event-bracketed sample of launches inside the timed region.
-    hbm, peak_kind = peaks()
-    if args.mc_mode == "graph":
-        upd_ms, upd_n = timing["update"]
-        kernel = "k_update (accept-and-update; bytes averaged over all launches, rejected moves move none)"
-        bytes_per_launch = work[1] / (M * args.steps)
-    else:
-        upd_ms, upd_n = timing["mc"]
-        kernel = ("k_mc (persistent Metropolis: dE reads + accept-and-update read-modify-writes, "
-                  f"{M} moves per launch)")
-        bytes_per_launch = (work[1] + work[2]) / max(upd_n, 1)
-    achieved = bytes_per_launch / (upd_ms / upd_n / 1e3) / 1e9 if upd_n else None
-    # DRAM traffic of k_mc from one ncu capture of a 256-move launch on this
-    # workload (966 MB read + 1 322 MB written), scaled to a launch by moves
-    traffic = None if args.mc_mode == "graph" else (966.42e6 + 1321.68e6) / 256 * M
+    clk_path = os.path.join(tempfile.gettempdir(), f"pdmk_clocks_rank{rank}_{os.getpid()}.csv")
 
-    # end to end through the C-ABI with host buffers (copies inside the timed region)
-    e2e_t = []
-    h2d = M * (8 + 24 + 8)
-    d2h = M * (8 + 4)
+    # FP64 Ewald energies of the systems, outside the timed region: the
+    # library's GPU Ewald (checked against the oracle's CPU Ewald to 1e-10 by
+    # the tests) at N = 1e6, the stored CPU value at N = 1e5
+    def gpu_ewald(r, q, WW):
+        t = P.HPDMKPtTree(P.HPDMKParams(n_per_leaf=WW["n_per_leaf"], digits=WW["digits"], L=WW["L"],
+                                        init=P.DIRECT), r, q, leaf_slack=0)
+        try:
+            return t.ewald_energy()[0]
+        finally:
+            t.close()
+
+    r, q = make_system(1 + rank, n, L)
+    ew_uniform = gpu_ewald(r, q, W)
+    with Clocks(clk_path) as clk:
+        arms, launches = run_system(P, torch, W, r, q, args, ws, l2_flush, seed=1 + rank, cand=W["candidates"],
+                                    with_timing=True)
+        mixed = arms["mixed"]
+        timing = mixed.tree.get_timing()
+        mixed.tree.set_timing(False)
+    res = {k: a.summary(ws, ew_uniform) for k, a in arms.items()}
+    M = W["moves_per_step"]
+    steps_time = sum(float(np.sum(a.t_moves) + np.sum(a.t_energy) + np.sum(a.t_cand)) for a in arms.values())
+
+    # roofline of the dominant kernel of the step: k_mc (persistent
+    # Metropolis) of the mixed arm, HBM bound; algorithmic bytes from the
+    # device work counters (dE reads + update read-modify-writes) over its
+    # CUDA-event duration on the tree's stream
+    hbm, peak_kind = peaks()
+    mc_ms, mc_n = timing["mc"]
+    bytes_per_launch = (mixed.work[1] + mixed.work[2]) / max(mc_n, 1)
+    achieved = bytes_per_launch / (mc_ms / mc_n / 1e3) / 1e9 if mc_n else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "k_mc_traffic_uniform_n1e6_d9.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath))["dram_bytes_per_move"] * M
+
+    # end to end through the C-ABI with host buffers, mixed path: the moves
+    # (hpdmk_mc_run: indices, displacements and uniforms in, shifts and
+    # decisions out) and the full energy (hpdmk_tree_init from host positions
+    # and charges, outgoing, incoming, energy, the energy read back)
+    e2e_t, e2e_e = [], []
     hidx, hdisp, hu = make_moves(99 + rank, n, M * args.steps, W["step"])
+    params = mixed.params
     for s in range(args.steps):
         barrier(ws)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        tree.mc_run(hidx[s * M:(s + 1) * M], hdisp[s * M:(s + 1) * M], hu[s * M:(s + 1) * M], W["beta"])
+        mixed.tree.mc_run(hidx[s * M:(s + 1) * M], hdisp[s * M:(s + 1) * M], hu[s * M:(s + 1) * M], W["beta"])
         e2e_t.append(time.perf_counter() - t0)
+        barrier(ws)
+        t0 = time.perf_counter()
+        t = P.HPDMKPtTree(params, r, q, leaf_slack=0, precision=P.PRECISION_MIXED)
+        t.form_outgoing_pw()
+        t.form_incoming_pw()
+        t.eval_energy()
+        e2e_e.append(time.perf_counter() - t0)
+        t.close()
     te2e = all_max(float(np.sum(e2e_t)), ws)
-    e2e_val = ws * M * args.steps / te2e
+    tee = all_max(float(np.sum(e2e_e)), ws)
+    for a in arms.values():
+        a.close()
+    del arms, mixed
+    torch.cuda.empty_cache()
 
-    # accuracy of the timed energy against the stored FP64 Ewald energy of
-    # this workload (tests/golden/bench_ewald.json, made by the oracle)
-    accuracy = None
+    # the clustered system (adaptive tree of depth 8)
+    rc, qc = make_clustered(5 + rank, CLUSTERED["N"], CLUSTERED["L"])
+    ew_cl = gpu_ewald(rc, qc, CLUSTERED)
+    cargs = argparse.Namespace(**vars(args))
+    cargs.steps = min(args.steps, 3)
+    carms, _ = run_system(P, torch, CLUSTERED, rc, qc, cargs, ws, l2_flush, seed=5 + rank, cand=0)
+    clustered = {k: a.summary(ws, ew_cl) for k, a in carms.items()}
+    clustered["mixed_vs_fp64"] = {"full_energy": clustered["mixed"]["full_energy_evals_per_s"] /
+                                  clustered["fp64"]["full_energy_evals_per_s"],
+                                  "moves": clustered["mixed"]["moves_per_s"] / clustered["fp64"]["moves_per_s"]}
+    clustered["config"] = dict(CLUSTERED, steps=cargs.steps)
+    for a in carms.values():
+        a.close()
+    del carms
+    torch.cuda.empty_cache()
+
+    # the N = 1e5 cube, against the stored CPU Ewald energy
+    W5 = dict(WORKLOAD_N1E5)
+    r5, q5 = make_system(1, W5["N"], W5["L"])
+    ew5 = None
     gp = os.path.join(ROOT, "tests", "golden", "bench_ewald.json")
-    if rank == 0 and os.path.exists(gp):
+    if os.path.exists(gp):
         g = json.load(open(gp))
-        if g["workload"]["N"] == n and g["workload"]["L"] == L and g["workload"]["seed"] == 1:
-            ew = g["ewald"]["energy"]
-            accuracy = {"energy_dmk": e_dmk, "energy_ewald_fp64": ew, "rel_err": abs(e_dmk - ew) / abs(ew),
-                        "ewald": "oracle FP64 Ewald, s = 5, stored"}
+        if g["workload"]["N"] == W5["N"] and g["workload"]["L"] == W5["L"] and g["workload"]["seed"] == 1:
+            ew5 = g["ewald"]["energy"]
+    a5, _ = run_system(P, torch, W5, r5, q5, cargs, ws, l2_flush, seed=1, cand=0)
+    n1e5 = {k: a.summary(ws, ew5) for k, a in a5.items()}
+    n1e5["mixed_vs_fp64"] = {"full_energy": n1e5["mixed"]["full_energy_evals_per_s"] /
+                             n1e5["fp64"]["full_energy_evals_per_s"]}
+    n1e5["config"] = dict(W5, steps=cargs.steps, ewald="oracle CPU FP64 Ewald, s = 5, stored")
+    for a in a5.values():
+        a.close()
+    del a5
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        res = cpu_baseline_sample(W)
-        cpu = {"value": res["moves_per_s"], "unit": "moves/s", "cores": 1, "kind": "port",
-               "sample": f"{res['moves']} sequential Metropolis moves of the oracle port (1 thread, as the "
-                         f"reference times moves) on the same workload; its full energy "
-                         f"{res['energy_evals_per_s']:.4g} evals/s on {res['cores']} threads",
-               "full_energy_evals_per_s": res["energy_evals_per_s"]}
+        cb = cpu_baseline_sample(W)
+        cpu = {"value": cb["moves_per_s"], "unit": "moves/s", "cores": 1, "kind": "port",
+               "sample": f"{cb['moves']} sequential Metropolis moves of the oracle port (1 thread, as the "
+                         f"reference times moves) on the same N = 1e6 workload; its full energy "
+                         f"{cb['energy_evals_per_s']:.4g} evals/s on {cb['cores']} threads",
+               "full_energy_evals_per_s": cb["energy_evals_per_s"]}
     if rank == 0:
         c = clk.summary(dev)
+        m, f = res["mixed"], res["fp64"]
         line = {
-            "metric": METRIC, "value": moves_per_s, "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * (tm + te) / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(W, parallelism="replicas" if ws > 1 else "single", mc_mode=args.mc_mode,
-                           l2="256 MB written before each step; the 0.56 GB of expansions exceed the 126 MB L2"),
-            "full_energy_evals_per_s": energy_per_s,
-            "accept_rate": work[0] / (M * args.steps),
-            "accuracy": accuracy,
+            "metric": METRIC, "value": m["moves_per_s"], "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * steps_time / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64+i8", "data": "synthetic",
+            "config": dict(W, parallelism="replicas" if ws > 1 else "single",
+                           value="mixed-precision path, 10^4 sequential Metropolis moves per step",
+                           l2="256 MB written before each timed phase; the 4.5 GB of expansions exceed the "
+                              "126 MB L2"),
+            "full_energy_evals_per_s": m["full_energy_evals_per_s"],
+            "mixed": m, "fp64": f,
+            "mixed_vs_fp64": {"moves": m["moves_per_s"] / f["moves_per_s"],
+                              "full_energy": m["full_energy_evals_per_s"] / f["full_energy_evals_per_s"],
+                              "candidates": m["candidates_per_s"] / f["candidates_per_s"]},
+            "accuracy": {"ewald_fp64": ew_uniform, "mixed_rel_err": m["rel_err_vs_ewald"],
+                         "fp64_rel_err": f["rel_err_vs_ewald"],
+                         "ewald": "the library's GPU FP64 Ewald (s = 5), checked against the oracle's CPU Ewald "
+                                  "to 1e-10 by the tests"},
+            "clustered": clustered,
+            "n1e5": n1e5,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 256-move k_mc "
-                                           "launch, scaled by moves per launch" if traffic else None,
-                         "kernel": kernel,
-                         "timed_launches": int(upd_n),
-                         "peak_source": peak_kind},
+                                           "launch on this workload, scaled by moves per launch" if traffic else None,
+                         "kernel": f"k_mc (persistent Metropolis, mixed arm: dE reads + accept-and-update "
+                                   f"read-modify-writes, {M} moves per launch)",
+                         "timed_launches": int(mc_n), "peak_source": peak_kind},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_val, "unit": "moves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": ws * M * args.steps / te2e, "unit": "moves/s", "h2d_bytes_per_step": M * (8 + 24 + 8),
+                    "d2h_bytes_per_step": M * (8 + 4),
+                    "full_energy_evals_per_s": ws * args.steps / tee,
+                    "full_energy_h2d_bytes": n * 32, "full_energy_d2h_bytes": 8,
+                    "path": "mixed precision through hpdmk_mc_run and hpdmk_tree_init + outgoing + incoming + "
+                            "energy with host arrays"},
             "gpu_launches": int(launches),
             "clocks": c,
         }
         print(json.dumps(line), flush=True)
-    tree.close()
+
+
+def run_profile(args):
+    """A short run for profilers (never a bench line): `reps` full energies
+    from HBM-resident positions and one Metropolis run of --moves-per-step
+    moves, for one precision on one workload."""
+    import torch
+    import pdmk4mc_b200 as P
+    W = dict(WORKLOAD_N1E5 if args.profile == "n1e5" else WORKLOAD)
+    prec = P.PRECISION_MIXED if args.precision == "mixed" else P.PRECISION_FP64
+    r, q = make_system(1, W["N"], W["L"])
+    params = P.HPDMKParams(n_per_leaf=W["n_per_leaf"], digits=W["digits"], L=W["L"], init=P.DIRECT)
+    d_r = torch.tensor(r, dtype=torch.float64, device="cuda")
+    d_q = torch.tensor(q, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    e = None
+    for _ in range(args.reps):
+        t = P.HPDMKPtTree(params, None, None, leaf_slack=8, device_inputs=(d_r.data_ptr(), d_q.data_ptr(), W["N"]),
+                          precision=prec)
+        t.form_outgoing_pw()
+        t.form_incoming_pw()
+        e = t.eval_energy()
+        t.close()
+    M = args.moves_per_step
+    if M > 0:
+        t = P.HPDMKPtTree(params, r, q, leaf_slack=8, precision=prec)
+        if args.mc_graph:
+            t.set_mc_mode(P.MC_GRAPH)
+        t.form_outgoing_pw()
+        t.form_incoming_pw()
+        idx, disp, u = make_moves(1, W["N"], M, W["step"])
+        t.mc_run(idx, disp, u, W["beta"])
+        t.close()
+    print(f"profile run done: {args.profile} {args.precision} E={e!r}")
 
 
 def main():
@@ -362,10 +583,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mc-mode", default="persistent", choices=["persistent", "graph"])
     ap.add_argument("--moves-per-step", type=int, default=WORKLOAD["moves_per_step"],
                     help="smaller values only for profiler runs; the reported workload uses the default")
+    ap.add_argument("--profile", choices=["n1e5", "n1e6"], default=None,
+                    help="a short run for profilers on one workload (prints no bench line)")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--mc-graph", action="store_true",
+                    help="profile runs: Metropolis moves as graphs of (k_shift, k_update) launches")
     args = ap.parse_args()
+    if args.profile:
+        run_profile(args)
+        return
     rank, ws = dist_init()
     try:
         if args.impl == "reference":

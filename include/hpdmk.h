@@ -143,6 +143,11 @@ int hpdmk_update_shift(hpdmk_tree tree, long i, double dx, double dy, double dz)
  * current state; no state change. Host arrays. */
 int hpdmk_eval_shift_energy_batch(hpdmk_tree tree, int m, const long *i, const double *d, double *dE);
 
+/* As hpdmk_eval_shift_energy_batch with device-resident int32 indices d_i[m],
+ * displacements d_d[3m] and output d_dE[m], enqueued on the tree's stream
+ * without a host synchronisation (one launch, one thread block per candidate). */
+int hpdmk_eval_shift_energy_batch_device(hpdmk_tree tree, int m, const int *d_i, const double *d_d, double *d_dE);
+
 /* No reference counterpart. Same results as hpdmk_eval_shift_energy_batch, but
  * the call allocates no device memory: its block partials, completion counter,
  * proposal record, phase tables and staged inputs/outputs live in one fixed
@@ -248,6 +253,14 @@ int hpdmk_get_update_bytes(hpdmk_tree tree, double *out);
 /* Kernel launches this library has issued since it was loaded, kernels run
  * inside its captured CUDA graphs included (no reference counterpart). */
 int hpdmk_get_launch_count(long long *out);
+
+/* Reference: read_particle_info (src/utils.cpp:14-28). Reads a text file
+ * whose first line is a header and whose further lines hold "x y z q"
+ * (whitespace-separated; lines that do not start with four numbers are
+ * skipped). *n receives the number of particles. With r and q both NULL the
+ * call only counts; otherwise r[3 n] (xyz-interleaved) and q[n] are filled,
+ * and capacity (particles) must be at least *n. Host only, no device work. */
+int hpdmk_read_particle_info(const char *filename, long *n, double *r, double *q, long capacity);
 
 /* Last status of the calling thread and its message. */
 int hpdmk_last_error(void);

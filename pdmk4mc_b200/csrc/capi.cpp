@@ -17,6 +17,10 @@
 #include "../../include/hpdmk.h"
 #include "tree.hpp"
 
+namespace pdmk {
+bool read_particle_info(const std::string& filename, std::vector<double>& xyzq);
+}
+
 namespace {
 
 thread_local int g_last_error = HPDMK_OK;
@@ -336,6 +340,16 @@ int hpdmk_eval_shift_energy_batch(hpdmk_tree t, int m, const long* i, const doub
   });
 }
 
+int hpdmk_eval_shift_energy_batch_device(hpdmk_tree t, int m, const int* d_i, const double* d_d, double* d_dE) {
+  if (!t || m < 0 || (m > 0 && (!d_i || !d_d || !d_dE))) return fail(HPDMK_ERR_BAD_INPUT, "bad batch arguments");
+  if (m == 0) return ok();
+  return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
+    H(t)->tree->shift_batch_device(m, d_i, d_d, d_dE);
+    return ok();
+  });
+}
+
 int hpdmk_mc_run(hpdmk_tree t, int n, const long* i, const double* d, const double* u, double beta, double* dE,
                  int* accepted) {
   if (!t || n < 0 || (n > 0 && (!i || !d || !u))) return fail(HPDMK_ERR_BAD_INPUT, "bad move arguments");
@@ -574,6 +588,29 @@ int hpdmk_get_update_bytes(hpdmk_tree t, double* out) {
   return guarded([&]() {
     DeviceGuard dg(H(t)->device);
     H(t)->tree->get_work(out);
+    return ok();
+  });
+}
+
+int hpdmk_read_particle_info(const char* filename, long* n, double* r, double* q, long capacity) {
+  if (!filename || !n) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  return guarded([&]() {
+    std::vector<double> xyzq;
+    if (!pdmk::read_particle_info(filename, xyzq))
+      return fail(HPDMK_ERR_BAD_INPUT, std::string("cannot open particle file ") + filename);
+    const long m = long(xyzq.size() / 4);
+    *n = m;
+    if (!r && !q) return ok();  // size query
+    if (!r || !q) return fail(HPDMK_ERR_BAD_INPUT, "need both r and q, or neither for a size query");
+    if (capacity < m)
+      return fail(HPDMK_ERR_BAD_INPUT, "particle file holds " + std::to_string(m) + " particles, capacity is " +
+                                           std::to_string(capacity));
+    for (long i = 0; i < m; ++i) {
+      r[3 * i] = xyzq[4 * i];
+      r[3 * i + 1] = xyzq[4 * i + 1];
+      r[3 * i + 2] = xyzq[4 * i + 2];
+      q[i] = xyzq[4 * i + 3];
+    }
     return ok();
   });
 }

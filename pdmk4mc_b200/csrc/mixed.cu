@@ -12,17 +12,19 @@
 // is one real matrix product over K = 2 x (particles):
 //   [Re | Im](rows x 2d) = [Ar Ai](rows x 2K) . [[Br, Bi], [-Bi, Br]](2K x 2d).
 // Both operands lie in [-1, 1] after the scaling below, so each is written in
-// fixed point as three signed 7-bit slices, t = a1 + a2 2^-7 + a3 2^-14
-// (|a_s| <= 64, truncation 2^-21 of the operand's range). The six slice
-// products with s + t <= 4 run as tcgen05.mma kind::i8 (int8 x int8 into
-// exact int32 accumulators in TMEM): acc0 = a1 b1, acc1 = a1 b2 + a2 b1,
-// acc2 = a1 b3 + a2 b2 + a3 b1. Integer accumulation is exact, so the sum
-// over a box's particles adds no rounding at all; the three accumulators
-// are combined in FP64 at the end, out = qmax 2^-12 (acc0 + 2^-7 acc1 +
-// 2^-14 acc2). This is the slice splitting of Ozaki, Ogita and Oishi (error-
-// free splitting of floating-point products) in the fixed-point form of
-// Ootomo, Ozaki and Yokota (DGEMM on integer matrix multiplication units,
-// 2024), applied to operands bounded by one.
+// fixed point, t = 127 v, as three signed 8-bit slices in base 254,
+// t = a1 + a2 / 254 + a3 / 254^2 (|a_s| <= 127; truncation 0.5 / 254^2 of t,
+// 6e-8 of the operand's range, about the FP32 rounding of the operand
+// itself). The six slice products with s + t <= 4 run as tcgen05.mma
+// kind::i8 (int8 x int8 into exact int32 accumulators in TMEM):
+// acc0 = a1 b1, acc1 = a1 b2 + a2 b1, acc2 = a1 b3 + a2 b2 + a3 b1. Integer
+// accumulation is exact, so the sum over a box's particles adds no rounding
+// at all; the three accumulators are combined in FP64 at the end,
+// out = qmax / 127^2 (acc0 + acc1 / 254 + acc2 / 254^2). This is the slice
+// splitting of Ozaki, Ogita and Oishi (error-free splitting of floating-point
+// products) in the fixed-point form of Ootomo, Ozaki and Yokota (DGEMM on
+// integer matrix multiplication units, 2024), applied to operands bounded by
+// one.
 //
 // One CTA computes up to two 128-row M tiles of one box (or split-K chunk of
 // a box) and streams the box's particles through shared memory 32 at a time:
@@ -96,19 +98,38 @@ struct MixShape {
 // named barrier ids
 constexpr int BAR_FULL0 = 1, BAR_EMPTY0 = 3, BAR_CONS = 5, BAR_PROD = 6;
 
-// t in [-64, 64] -> three float words whose low bytes are the signed 7-bit
-// slices a1, a2, a3 with t = a1 + a2 / 128 + a3 / 16384 + e, |e| <= 2^-15.
-// Adding 1.5 * 2^23 rounds to an integer that lands in the low mantissa bits.
-__device__ __forceinline__ void slice3(float t, uint32_t& s1, uint32_t& s2, uint32_t& s3) {
-  const float MAG = 12582912.0f;
-  const float f1 = t + MAG;
-  const float r1 = t - (f1 - MAG);
-  const float f2 = fmaf(r1, 128.0f, MAG);
-  const float r2 = fmaf(r1, 128.0f, -(f2 - MAG));
-  const float f3 = fmaf(r2, 128.0f, MAG);
-  s1 = __float_as_uint(f1);
-  s2 = __float_as_uint(f2);
-  s3 = __float_as_uint(f3);
+constexpr float SL_BASE = 254.0f;  // slice base; operands are scaled to |t| <= 127
+constexpr double SL_SCALE = 127.0;
+
+// t in [-127, 127] -> three float words whose low bytes are the signed 8-bit
+// slices a1, a2, a3 with t = a1 + a2 / 254 + a3 / 254^2 + e, |e| <= 0.5 / 254^2,
+// for a pair of values (the real and imaginary part of one complex operand)
+// with the paired FP32 instructions of sm_100 (one issue slot for both lanes,
+// each lane rounded as its scalar instruction). Adding MAG = 1.5 * 2^23
+// rounds to an integer that lands in the low mantissa bits; -round(t) =
+// MAG - (t + MAG) is exact, t - a1 is exact, and each FMA forms r * 254 - a
+// exactly before its one rounding.
+__device__ __forceinline__ void slice3x2(float2 t, uint32_t (&re)[3], uint32_t (&im)[3]) {
+  const float2 MAG2 = make_float2(12582912.0f, 12582912.0f);
+  const float2 NEG1 = make_float2(-1.0f, -1.0f);
+  const float2 B2 = make_float2(SL_BASE, SL_BASE);
+  const float2 f1 = __fadd2_rn(t, MAG2);
+  const float2 r1 = __fadd2_rn(t, __ffma2_rn(f1, NEG1, MAG2));
+  const float2 f2 = __ffma2_rn(r1, B2, MAG2);
+  const float2 r2 = __ffma2_rn(r1, B2, __ffma2_rn(f2, NEG1, MAG2));
+  const float2 f3 = __ffma2_rn(r2, B2, MAG2);
+  re[0] = __float_as_uint(f1.x);
+  re[1] = __float_as_uint(f2.x);
+  re[2] = __float_as_uint(f3.x);
+  im[0] = __float_as_uint(f1.y);
+  im[1] = __float_as_uint(f2.y);
+  im[2] = __float_as_uint(f3.y);
+}
+
+// z y for complex FP32 operands with two paired instructions
+__device__ __forceinline__ float2 cmul_x2(float2 z, float2 y) {
+  const float2 p = __fmul2_rn(make_float2(z.x, z.x), y);               // (zr yr, zr yi)
+  return __ffma2_rn(make_float2(-z.y, z.y), make_float2(y.y, y.x), p);  // (zr yr - zi yi, zr yi + zi yr)
 }
 
 // low bytes of four words -> one word [x0.b0, x1.b0, x2.b0, x3.b0]
@@ -250,7 +271,7 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
           const double xa = P[a * COORD_BOX + off + j];
           const double ca = a == 0 ? it.cx : (a == 1 ? it.cy : it.cz);
           const int Xa = a == 0 ? it.X : (a == 1 ? it.Y : it.Z);
-          const double scale = a == 0 ? 64.0 : (a == 1 ? 1.0 : 64.0 * P[3 * COORD_BOX + off + j] * inv_qmax);
+          const double scale = a == 0 ? SL_SCALE : (a == 1 ? 1.0 : SL_SCALE * P[3 * COORD_BOX + off + j] * inv_qmax);
           axis_factors_f32(xa - ca, it.dk, it.M, Xa, NK, len, scale, dst);
         } else {
           for (int m = 0; m < len; ++m) dst[m] = make_float2(0.f, 0.f);
@@ -275,20 +296,18 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
           const int j0 = kc * 8 + 2 * p;
-          float v[4] = {0.f, 0.f, 0.f, 0.f};
+          float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
           if (re || im) {
             const float2 e0 = ex[j0 * D + kx], e1 = ex[(j0 + 1) * D + kx];
-            // real output column: (Br, -Bi); imaginary: (Bi, Br)
-            v[0] = re ? e0.x : e0.y;
-            v[1] = re ? -e0.y : e0.x;
-            v[2] = re ? e1.x : e1.y;
-            v[3] = re ? -e1.y : e1.x;
+            // K rows (2j, 2j+1) of a real output column: (Br, -Bi); of an imaginary one: (Bi, Br)
+            v0 = re ? make_float2(e0.x, -e0.y) : make_float2(e0.y, e0.x);
+            v1 = re ? make_float2(e1.x, -e1.y) : make_float2(e1.y, e1.x);
           }
-          uint32_t a[4][3];
+          uint32_t a0[3], b0[3], a1[3], b1[3];
+          slice3x2(v0, a0, b0);
+          slice3x2(v1, a1, b1);
 #pragma unroll
-          for (int q = 0; q < 4; ++q) slice3(v[q], a[q][0], a[q][1], a[q][2]);
-#pragma unroll
-          for (int sl = 0; sl < 3; ++sl) w[sl][p] = pack4(a[0][sl], a[1][sl], a[2][sl], a[3][sl]);
+          for (int sl = 0; sl < 3; ++sl) w[sl][p] = pack4(a0[sl], b0[sl], a1[sl], b1[sl]);
         }
 #pragma unroll
         for (int sl = 0; sl < 3; ++sl)
@@ -319,17 +338,13 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
 #pragma unroll
           for (int p = 0; p < 4; ++p) {
             const int j0 = kc * 8 + 2 * p;
-            const float2 z0 = ez[j0 * (NK + 1) + kz], y0 = ey[j0 * D + ky];
-            const float2 z1 = ez[(j0 + 1) * (NK + 1) + kz], y1 = ey[(j0 + 1) * D + ky];
-            const float v0r = fmaf(z0.x, y0.x, -z0.y * y0.y), v0i = fmaf(z0.x, y0.y, z0.y * y0.x);
-            const float v1r = fmaf(z1.x, y1.x, -z1.y * y1.y), v1i = fmaf(z1.x, y1.y, z1.y * y1.x);
-            uint32_t a[4][3];
-            slice3(v0r, a[0][0], a[0][1], a[0][2]);
-            slice3(v0i, a[1][0], a[1][1], a[1][2]);
-            slice3(v1r, a[2][0], a[2][1], a[2][2]);
-            slice3(v1i, a[3][0], a[3][1], a[3][2]);
+            const float2 v0 = cmul_x2(ez[j0 * (NK + 1) + kz], ey[j0 * D + ky]);
+            const float2 v1 = cmul_x2(ez[(j0 + 1) * (NK + 1) + kz], ey[(j0 + 1) * D + ky]);
+            uint32_t a0r[3], a0i[3], a1r[3], a1i[3];
+            slice3x2(v0, a0r, a0i);
+            slice3x2(v1, a1r, a1i);
 #pragma unroll
-            for (int sl = 0; sl < 3; ++sl) w[sl][p] = pack4(a[0][sl], a[1][sl], a[2][sl], a[3][sl]);
+            for (int sl = 0; sl < 3; ++sl) w[sl][p] = pack4(a0r[sl], a0i[sl], a1r[sl], a1i[sl]);
           }
 #pragma unroll
           for (int sl = 0; sl < 3; ++sl)
@@ -380,7 +395,7 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
     const int q = warp & 3;       // TMEM lane quarter
     const int lt = lr & 127;      // row within the tile
     double2* stage = reinterpret_cast<double2*>(sm) + size_t(t * 128 + lt) * D;
-    const double scale = qmax * (1.0 / 4096.0);
+    const double scale = qmax / (SL_SCALE * SL_SCALE);
     if (t * 128 < nrows) {
       if (nch > 0 && !s_abort) {
 #pragma unroll 1
@@ -394,8 +409,8 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
 #pragma unroll
           for (int k = 0; k < 16; ++k) {
             const int n = cb * 16 + k;
-            const double v =
-                scale * fma(double(int(r2[k])), 1.0 / 16384.0, fma(double(int(r1[k])), 1.0 / 128.0, double(int(r0[k]))));
+            const double v = scale * fma(double(int(r2[k])), 1.0 / (254.0 * 254.0),
+                                         fma(double(int(r1[k])), 1.0 / 254.0, double(int(r0[k]))));
             if (n < D) stage[n].x = v;
             else if (n >= HALF && n < HALF + D) reinterpret_cast<double*>(stage + (n - HALF))[1] = v;
           }

@@ -98,6 +98,19 @@ def replicas_energy(trees):
     return e
 
 
+def read_particle_info(path):
+    """The reference's read_particle_info (src/utils.cpp:14-28): a header line,
+    then "x y z q" per line. Returns (r[3n] xyz-interleaved, q[n])."""
+    L = load_library()
+    n = ctypes.c_long(0)
+    p = os.fsencode(path)
+    _check(L.hpdmk_read_particle_info(p, ctypes.byref(n), None, None, 0))
+    r = np.zeros(3 * n.value)
+    q = np.zeros(n.value)
+    _check(L.hpdmk_read_particle_info(p, ctypes.byref(n), _p(r), _p(q), n.value))
+    return r, q
+
+
 def load_library():
     global _LIB
     if _LIB is not None:
@@ -161,6 +174,9 @@ def load_library():
     L.hpdmk_eval_shift_energy_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp]
     L.hpdmk_eval_shift_energy_batch_static.restype = ctypes.c_int
     L.hpdmk_eval_shift_energy_batch_static.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp]
+    L.hpdmk_eval_shift_energy_batch_device.restype = ctypes.c_int
+    L.hpdmk_eval_shift_energy_batch_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p]
     L.hpdmk_mc_run.restype = ctypes.c_int
     L.hpdmk_mc_run.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp, ctypes.c_double, _dp, _ip]
     L.hpdmk_mc_run_device.restype = ctypes.c_int
@@ -170,6 +186,8 @@ def load_library():
     L.hpdmk_get_positions.argtypes = [ctypes.c_void_p, _dp]
     L.hpdmk_tree_info.restype = ctypes.c_int
     L.hpdmk_tree_info.argtypes = [ctypes.c_void_p, _lp]
+    L.hpdmk_read_particle_info.restype = ctypes.c_int
+    L.hpdmk_read_particle_info.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_long), _dp, _dp, ctypes.c_long]
     L.hpdmk_last_error.restype = ctypes.c_int
     L.hpdmk_last_error.argtypes = []
     L.hpdmk_last_error_message.restype = ctypes.c_char_p
@@ -325,6 +343,10 @@ class HPDMKPtTree:
     def mc_run_device(self, n, d_idx_ptr, d_disp_ptr, d_u_ptr, beta, d_dE_ptr, d_acc_ptr):
         _check(load_library().hpdmk_mc_run_device(self._h, int(n), d_idx_ptr, d_disp_ptr, d_u_ptr, float(beta),
                                                   d_dE_ptr, d_acc_ptr))
+
+    def eval_shift_energy_batch_device(self, m, d_idx_ptr, d_disp_ptr, d_dE_ptr):
+        """Candidate batch on device arrays (int32 indices), enqueued on the tree's stream."""
+        _check(load_library().hpdmk_eval_shift_energy_batch_device(self._h, int(m), d_idx_ptr, d_disp_ptr, d_dE_ptr))
 
     def synchronize(self):
         _check(load_library().hpdmk_synchronize(self._h))

@@ -18,7 +18,7 @@ from oracle import oracle as O  # noqa: E402
 
 
 def main():
-    W = bench.WORKLOAD
+    W = bench.WORKLOAD_N1E5
     r, q = bench.make_system(1, W["N"], W["L"])
     e = O.ewald_energy(W["L"], r, q, s=5.0, alpha=0.4)
     out = {"workload": {"N": W["N"], "L": W["L"], "seed": 1, "charges": "alternating +1/-1"},

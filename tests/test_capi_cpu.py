@@ -91,3 +91,20 @@ def test_host_prolate_setup_matches_reference(digits):
     assert abs(c0r - G[f"d{digits}_C0"] / p0) < 1e-13
     assert abs(diff0 / G[f"d{digits}_diff0"] - 1) < 1e-12
     np.testing.assert_allclose(psi, G[f"d{digits}_psi0"] / p0, rtol=0, atol=1e-14)
+
+
+def test_read_particle_info(tmp_path):
+    # the reference's read_particle_info (src/utils.cpp:14-28): the first line
+    # is a header; a line counts when it starts with four numbers x y z q
+    f = tmp_path / "system.xyzq"
+    f.write_text("x y z q\n1.5 2 3 1\nnot a particle\n4 5 6 -1 trailing words\n\n7 8\n0.25 0.5 0.75 2e-1\n")
+    r, q = P.read_particle_info(str(f))
+    np.testing.assert_array_equal(r, [1.5, 2, 3, 4, 5, 6, 0.25, 0.5, 0.75])
+    np.testing.assert_array_equal(q, [1, -1, 0.2])
+    g = tmp_path / "header_only.xyzq"
+    g.write_text("x y z q\n")
+    r, q = P.read_particle_info(str(g))
+    assert r.size == 0 and q.size == 0
+    with pytest.raises(P.HPDMKError) as e:
+        P.read_particle_info(str(tmp_path / "missing.xyzq"))
+    assert e.value.code == 2

@@ -50,7 +50,7 @@ def test_gpu_ewald_bench_workload_and_dmk_error():
     sys.path.insert(0, os.path.dirname(HERE))
     import bench
     g = json.load(open(os.path.join(HERE, "golden", "bench_ewald.json")))
-    W = bench.WORKLOAD
+    W = bench.WORKLOAD_N1E5
     r, q = bench.make_system(1, W["N"], W["L"])
     t = P.HPDMKPtTree(P.HPDMKParams(n_per_leaf=W["n_per_leaf"], digits=W["digits"], L=W["L"], init=P.DIRECT), r, q)
     try:
