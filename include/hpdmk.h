@@ -250,6 +250,24 @@ int hpdmk_get_timing(hpdmk_tree tree, double *out, int reset);
  * out[2] algorithmic bytes read by the dE evaluations of the persistent kernel. */
 int hpdmk_get_update_bytes(hpdmk_tree tree, double *out);
 
+/* Autotuner (no reference counterpart): times the energy pipeline of this
+ * tree over candidate run-time splits and tiles, one parameter at a time,
+ * with CUDA events on the tree's stream, keeps the fastest and records them
+ * per (digits, precision, floor(log2 N)) in the JSON table at `path` (NULL
+ * or "": tuning.json beside the library, or the file named by the
+ * environment variable HPDMK_TUNING). New trees read that table. The
+ * parameters, chosen[0..3]: particles per split-K chunk of a box in the
+ * outgoing pass, particles per chunk of the root pass, resident waves of
+ * blocks in the incoming pass, most near-field target chunks per leaf;
+ * times[0..2] (may be NULL): outgoing, incoming and near-field milliseconds
+ * with the chosen values (medians of `reps` runs). The tree's expansions are
+ * left formed. */
+int hpdmk_autotune(hpdmk_tree tree, const char *path, int reps, int *chosen, double *times);
+/* The tree's current run-time splits and tiles (the four values above), and
+ * setting them by hand (values are clamped to the supported ranges). */
+int hpdmk_get_tuning(hpdmk_tree tree, int *out);
+int hpdmk_set_tuning(hpdmk_tree tree, const int *in);
+
 /* Kernel launches this library has issued since it was loaded, kernels run
  * inside its captured CUDA graphs included (no reference counterpart). */
 int hpdmk_get_launch_count(long long *out);
@@ -276,6 +294,8 @@ int hpdmk_debug_shift_parts(hpdmk_tree tree, long i, double dx, double dy, doubl
 /* Host-only PSWF set-up for a digits setting: out[0] c, out[1] lambda, out[2] C0 / psi0(0),
  * out[3] diff0, out[4] n_window, out[5] n_diff; psi[k] = psi0(x[k]) / psi0(0) for k < nx. */
 int hpdmk_debug_prolate(int digits, double *out, int nx, const double *x, double *psi);
+/* Host-only: the tuning a tree of (digits, precision, n) would read from the table file at path. */
+int hpdmk_debug_tuning_lookup(const char *path, int digits, int precision, long n, int *out);
 
 #ifdef __cplusplus
 }

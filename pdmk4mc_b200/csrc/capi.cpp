@@ -19,6 +19,9 @@
 
 namespace pdmk {
 bool read_particle_info(const std::string& filename, std::vector<double>& xyzq);
+Tuning lookup_tuning(int digits, int precision, long n);
+void autotune_tree(DmkTree& t, const char* path, int reps, int* out, double* times);
+Tuning lookup_tuning_file(const std::string& path, int digits, int precision, long n);
 }
 
 namespace {
@@ -189,6 +192,7 @@ hpdmk_tree init_impl(HPDMKParams params, const HPDMKExtParams* ext, int n, const
     hh->L = params.L;
     hh->tree = std::make_unique<pdmk::DmkTree>(params.L, params.n_per_leaf, params.digits, n, r, q, on_device, opt,
                                                hh->stream);
+    hh->tree->set_tuning(pdmk::lookup_tuning(params.digits, opt.precision, n));
     h = hh.release();
     return ok();
   });
@@ -556,6 +560,7 @@ int hpdmk_tree_rebuild(hpdmk_tree t) {
       auto nt = std::make_unique<pdmk::DmkTree>(old.box(), old.n_per_leaf(), old.digits(), n, d_r, d_q, true,
                                                 old.options(), h->stream);
       nt->set_mc_mode(old.mc_mode());  // the caller's settings carry over
+      nt->set_tuning(old.tuning());
       h->tree = std::move(nt);
     } catch (...) {
       cudaFreeAsync(d_r, h->stream);
@@ -573,6 +578,48 @@ int hpdmk_ewald_energy(hpdmk_tree t, double* energy, double* parts) {
   return guarded([&]() {
     DeviceGuard dg(H(t)->device);
     *energy = H(t)->tree->ewald_energy(parts);
+    return ok();
+  });
+}
+
+int hpdmk_autotune(hpdmk_tree t, const char* path, int reps, int* chosen, double* times) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
+    pdmk::autotune_tree(*H(t)->tree, path, reps, chosen, times);
+    return ok();
+  });
+}
+
+int hpdmk_get_tuning(hpdmk_tree t, int* out) {
+  if (!t || !out) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  const pdmk::Tuning& u = H(t)->tree->tuning();
+  out[0] = u.ksplit;
+  out[1] = u.ksplit_root;
+  out[2] = u.inc_waves;
+  out[3] = u.res_ny_max;
+  return ok();
+}
+
+int hpdmk_set_tuning(hpdmk_tree t, const int* in) {
+  if (!t || !in) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  pdmk::Tuning u;
+  u.ksplit = in[0];
+  u.ksplit_root = in[1];
+  u.inc_waves = in[2];
+  u.res_ny_max = in[3];
+  H(t)->tree->set_tuning(u);
+  return ok();
+}
+
+int hpdmk_debug_tuning_lookup(const char* path, int digits, int precision, long n, int* out) {
+  if (!path || !out) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  return guarded([&]() {
+    const pdmk::Tuning u = pdmk::lookup_tuning_file(path, digits, precision, n);
+    out[0] = u.ksplit;
+    out[1] = u.ksplit_root;
+    out[2] = u.inc_waves;
+    out[3] = u.res_ny_max;
     return ok();
   });
 }

@@ -806,13 +806,51 @@ __global__ void k_sum_q2(const double* sq, int n, double* out) {
 // ---------------------------------------------------------------------------
 // host side
 
-constexpr int KSPLIT = 4096;       // particles per split-K chunk of a box
-constexpr int KSPLIT_ROOT = 2048;  // particles per chunk of the root pass
+constexpr int RES_NY_MAX = 8;  // the partials buffer holds this many near-field chunks per node
 
 // target chunks per leaf in the near-field launch: enough for a full leaf
-// with its slack (larger leaves loop over their chunks)
+// with its slack (larger leaves loop over their chunks), at most the tuned cap
 int DmkTree::res_chunks() const {
-  return std::min(8, std::max(1, (n_per_leaf_ + opt_.leaf_slack + RES_TCH - 1) / RES_TCH));
+  return std::min(std::min(RES_NY_MAX, tune_.res_ny_max),
+                  std::max(1, (n_per_leaf_ + opt_.leaf_slack + RES_TCH - 1) / RES_TCH));
+}
+
+void DmkTree::set_tuning(const Tuning& t) {
+  Tuning c = t;
+  const int cap = opt_.precision == 1 ? 16384 : 1 << 20;
+  c.ksplit = std::min(cap, std::max(256, c.ksplit));
+  c.ksplit_root = std::min(cap, std::max(256, c.ksplit_root));
+  c.inc_waves = std::min(64, std::max(1, c.inc_waves));
+  c.res_ny_max = std::min(RES_NY_MAX, std::max(1, c.res_ny_max));
+  tune_ = c;
+}
+
+double DmkTree::time_phase(int phase, int reps) {
+  std::vector<float> ms;
+  cudaEvent_t a, b;
+  PDMK_CUDA(cudaEventCreate(&a));
+  PDMK_CUDA(cudaEventCreate(&b));
+  for (int r = 0; r < reps; ++r) {
+    PDMK_CUDA(cudaStreamSynchronize(st_));
+    PDMK_CUDA(cudaEventRecord(a, st_));
+    if (phase == 0) {
+      form_outgoing_pw();
+    } else if (phase == 1) {
+      form_incoming_pw();
+    } else {
+      ensure_packed();
+      launch_res_energy();
+    }
+    PDMK_CUDA(cudaEventRecord(b, st_));
+    PDMK_CUDA(cudaEventSynchronize(b));
+    float t = 0;
+    PDMK_CUDA(cudaEventElapsedTime(&t, a, b));
+    ms.push_back(t);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  std::sort(ms.begin(), ms.end());
+  return ms.empty() ? 0.0 : double(ms[ms.size() / 2]);
 }
 
 size_t DmkTree::partials_needed() const {
@@ -823,7 +861,7 @@ size_t DmkTree::partials_needed() const {
   need = std::max<size_t>(need, size_t(n_pw) * ktiles + 2 * size_t(n_pw) + 64);
   // sibling-tiled incoming: at most one group per 8 expansion boxes
   need = std::max<size_t>(need, size_t((D.H + INC_KT - 1) / INC_KT) * size_t(n_pw / 8 + 1) + 2 * size_t(n_pw) + 64);
-  need = std::max<size_t>(need, size_t(D.n_nodes) * res_chunks() + 64);
+  need = std::max<size_t>(need, size_t(D.n_nodes) * RES_NY_MAX + 64);
   return need;
 }
 
@@ -948,6 +986,7 @@ void DmkTree::form_outgoing_pw() {
   // Root pass first, on the second stream: the root (node 0, all slots) needs
   // no host view of the tree, so it runs while the host lays out the boxes.
   // Its allocations are made on the tree's stream before the fork event.
+  const int KSPLIT = tune_.ksplit, KSPLIT_ROOT = tune_.ksplit_root;
   const int nch_root = std::max(1, (D.n_slots + KSPLIT_ROOT - 1) / KSPLIT_ROOT);
   std::vector<Chunked> root_split{{0, nch_root, D.out_root}};
   double2* part_r = nullptr;
@@ -1146,7 +1185,7 @@ void DmkTree::run_incoming(bool write_inc) {
   if (write_inc) {
     // about four resident waves of blocks, each walking a strided set of tiles
     const int kt = (D.H + INC_KT - 1) / INC_KT;
-    const int slots = std::max(1, std::min(kt, (4 * 8 * 148 + n_groups_ - 1) / n_groups_));
+    const int slots = std::max(1, std::min(kt, (tune_.inc_waves * 8 * 148 + n_groups_ - 1) / n_groups_));
     k_incoming_sib<<<unsigned(slots * n_groups_), 8 * INC_KT, 0, st_>>>(D, d_groups_, n_groups_, slots, part);
     PDMK_LAUNCH_CHECK();
     k_diff_finish_sib<<<1, 1024, 0, st_>>>(D, d_groups_, n_groups_, slots, part, d_nonleaf_, n_nonleaf_, q2, d_Cl_,

@@ -182,6 +182,16 @@ struct EnergyParts {
 };
 
 
+// Run-time split and tile choices of the energy pipeline, picked per digits
+// setting, precision and size by the autotuner (tune.cpp) and cached in a
+// JSON table that trees read at construction.
+struct Tuning {
+  int ksplit = 4096;       // particles per split-K chunk of a box in the outgoing pass
+  int ksplit_root = 2048;  // particles per chunk of the root pass
+  int inc_waves = 4;       // resident waves of blocks (8 per SM) in the incoming pass
+  int res_ny_max = 8;      // most target chunks (64 targets each) per leaf in the near field
+};
+
 struct TreeOptions {
   int leaf_slack = 0;      // extra particle slots per leaf for moves
   int pool_capacity = 4096;
@@ -347,8 +357,16 @@ class DmkTree {
   // mixed precision: [0] max |q| (fixed-point scale), [1] error word (as int) of the tensor-core pass
   double* d_mix_ = nullptr;
   bool qmax_ready_ = false;
+  Tuning tune_;
  public:
   int precision() const { return opt_.precision; }
+  const Tuning& tuning() const { return tune_; }
+  // clamps to the supported ranges (the mixed pass's exact int32 sums bound
+  // a split-K chunk to 16384 particles)
+  void set_tuning(const Tuning& t);
+  // times one phase of the energy pipeline (0 outgoing, 1 incoming, 2 near
+  // field) `reps` times on the tree's stream; returns the median milliseconds
+  double time_phase(int phase, int reps);
   // error word of the mixed pass (nonzero: a pipeline wait gave up); synchronises
   int check_mixed_error();
 

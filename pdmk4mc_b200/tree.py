@@ -188,6 +188,14 @@ def load_library():
     L.hpdmk_tree_info.argtypes = [ctypes.c_void_p, _lp]
     L.hpdmk_read_particle_info.restype = ctypes.c_int
     L.hpdmk_read_particle_info.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_long), _dp, _dp, ctypes.c_long]
+    L.hpdmk_autotune.restype = ctypes.c_int
+    L.hpdmk_autotune.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, _ip, _dp]
+    L.hpdmk_get_tuning.restype = ctypes.c_int
+    L.hpdmk_get_tuning.argtypes = [ctypes.c_void_p, _ip]
+    L.hpdmk_set_tuning.restype = ctypes.c_int
+    L.hpdmk_set_tuning.argtypes = [ctypes.c_void_p, _ip]
+    L.hpdmk_debug_tuning_lookup.restype = ctypes.c_int
+    L.hpdmk_debug_tuning_lookup.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_long, _ip]
     L.hpdmk_last_error.restype = ctypes.c_int
     L.hpdmk_last_error.argtypes = []
     L.hpdmk_last_error_message.restype = ctypes.c_char_p
@@ -347,6 +355,30 @@ class HPDMKPtTree:
     def eval_shift_energy_batch_device(self, m, d_idx_ptr, d_disp_ptr, d_dE_ptr):
         """Candidate batch on device arrays (int32 indices), enqueued on the tree's stream."""
         _check(load_library().hpdmk_eval_shift_energy_batch_device(self._h, int(m), d_idx_ptr, d_disp_ptr, d_dE_ptr))
+
+    TUNING_FIELDS = ("ksplit", "ksplit_root", "inc_waves", "res_ny_max")
+
+    def autotune(self, path=None, reps=3):
+        """Search this tree's run-time splits and tiles and record them in the
+        tuning table (path None: tuning.json beside the library). Returns
+        (chosen {field: value}, {phase: milliseconds})."""
+        chosen = np.zeros(4, np.int32)
+        times = np.zeros(3)
+        p = os.fsencode(path) if path else None
+        _check(load_library().hpdmk_autotune(self._h, p, int(reps), _p(chosen, _ip), _p(times)))
+        return (dict(zip(self.TUNING_FIELDS, (int(v) for v in chosen))),
+                dict(zip(("outgoing_ms", "incoming_ms", "near_field_ms"), (float(v) for v in times))))
+
+    def tuning(self):
+        v = np.zeros(4, np.int32)
+        _check(load_library().hpdmk_get_tuning(self._h, _p(v, _ip)))
+        return dict(zip(self.TUNING_FIELDS, (int(x) for x in v)))
+
+    def set_tuning(self, **kw):
+        cur = self.tuning()
+        cur.update(kw)
+        v = np.array([cur[f] for f in self.TUNING_FIELDS], np.int32)
+        _check(load_library().hpdmk_set_tuning(self._h, _p(v, _ip)))
 
     def synchronize(self):
         _check(load_library().hpdmk_synchronize(self._h))

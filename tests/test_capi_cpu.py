@@ -108,3 +108,29 @@ def test_read_particle_info(tmp_path):
     with pytest.raises(P.HPDMKError) as e:
         P.read_particle_info(str(tmp_path / "missing.xyzq"))
     assert e.value.code == 2
+
+
+def test_tuning_table_lookup(tmp_path):
+    # the autotuner's JSON table: the same size bucket (floor(log2 N)) wins,
+    # else the nearest bucket of the same digits and precision, else defaults
+    f = tmp_path / "tuning.json"
+    f.write_text('[\n  {"digits": 9, "precision": 1, "n_log2": 16, "ksplit": 2048, "ksplit_root": 1024, '
+                 '"inc_waves": 8, "res_ny_max": 4},\n'
+                 '  {"digits": 9, "precision": 1, "n_log2": 19, "ksplit": 8192, "ksplit_root": 4096, '
+                 '"inc_waves": 2, "res_ny_max": 2},\n'
+                 '  {"digits": 9, "precision": 0, "n_log2": 19, "ksplit": 16384}\n]\n')
+    lib = P.load_library()
+    out = np.zeros(4, np.int32)
+
+    def look(d, p, n):
+        assert lib.hpdmk_debug_tuning_lookup(str(f).encode(), d, p, n, out.ctypes.data_as(
+            ctypes.POINTER(ctypes.c_int))) == 0
+        return out.tolist()
+    assert look(9, 1, 100000) == [2048, 1024, 8, 4]      # 2^16 <= 1e5 < 2^17
+    assert look(9, 1, 1000000) == [8192, 4096, 2, 2]     # 2^19 <= 1e6 < 2^20
+    assert look(9, 1, 4000000) == [8192, 4096, 2, 2]     # nearest bucket
+    assert look(9, 0, 1000000) == [16384, 2048, 4, 8]    # missing fields keep their defaults
+    assert look(6, 1, 1000000) == [4096, 2048, 4, 8]     # no entry: defaults
+    (tmp_path / "bad.json").write_text("not json at all {")
+    assert lib.hpdmk_debug_tuning_lookup(str(tmp_path / "bad.json").encode(), 9, 1, 1000, out.ctypes.data_as(
+        ctypes.POINTER(ctypes.c_int))) == 0 and out.tolist() == [4096, 2048, 4, 8]
