@@ -817,7 +817,10 @@ int DmkTree::res_chunks() const {
 
 void DmkTree::set_tuning(const Tuning& t) {
   Tuning c = t;
-  const int cap = opt_.precision == 1 ? 16384 : 1 << 20;
+  // the mixed pass's exact int32 sums hold at most 16384 particles per
+  // split-K chunk (four signed 8-bit slice products of up to 2^14 per
+  // accumulator and K entry, two K entries per particle); half of it is allowed
+  const int cap = opt_.precision == 1 ? 8192 : 1 << 20;
   c.ksplit = std::min(cap, std::max(256, c.ksplit));
   c.ksplit_root = std::min(cap, std::max(256, c.ksplit_root));
   c.inc_waves = std::min(64, std::max(1, c.inc_waves));
@@ -929,7 +932,7 @@ void DmkTree::form_outgoing_pw() {
     }
   };
   const bool mixed = opt_.precision == 1;
-  CUtensorMap tmap{};
+  CUtensorMap tmap_root{}, tmap_box{};
   if (mixed) {
     if (!d_mix_) {
       d_mix_ = static_cast<double*>(alloc(sizeof(double) * 2));
@@ -939,7 +942,8 @@ void DmkTree::form_outgoing_pw() {
       launch_absmax(D.sq, D.n_slots, d_mix_, st_);
       qmax_ready_ = true;
     }
-    make_coord_map(&tmap, D.sx, slot_capacity_);
+    make_coord_map(&tmap_root, D.sx, slot_capacity_, mixed_chunk(D.n_window));
+    make_coord_map(&tmap_box, D.sx, slot_capacity_, mixed_chunk(D.n_diff));
   }
   int* d_mix_err = mixed ? reinterpret_cast<int*>(d_mix_ + 1) : nullptr;
   auto align16 = [](size_t b) { return (b + 15) & ~size_t(15); };
@@ -1011,7 +1015,7 @@ void DmkTree::form_outgoing_pw() {
   PDMK_CUDA(cudaEventRecord(ev_fork_, st_));
   PDMK_CUDA(cudaStreamWaitEvent(aux_, ev_fork_, 0));
   if (mixed)
-    dispatch_mixed(D.n_window, tmap, reinterpret_cast<const MixItem*>(d_root), int(mroot.size()), d_mix_, d_mix_err,
+    dispatch_mixed(D.n_window, tmap_root, reinterpret_cast<const MixItem*>(d_root), int(mroot.size()), d_mix_, d_mix_err,
                    aux_);
   else
     dispatch_nudft(D.n_window, reinterpret_cast<const NudftWork*>(d_root), int(wroot.size()),
@@ -1098,7 +1102,7 @@ void DmkTree::form_outgoing_pw() {
   }
   time_begin(3);
   if (mixed)
-    dispatch_mixed(D.n_diff, tmap, reinterpret_cast<const MixItem*>(d_box), int(mbox.size()), d_mix_, d_mix_err,
+    dispatch_mixed(D.n_diff, tmap_box, reinterpret_cast<const MixItem*>(d_box), int(mbox.size()), d_mix_, d_mix_err,
                    st_);
   else
     dispatch_nudft(D.n_diff, reinterpret_cast<const NudftWork*>(d_box), int(wbox.size()),

@@ -6,8 +6,9 @@
 
 namespace pdmk {
 
-// One CTA of the mixed pass: M tiles `pair` (rows [pair * rows per CTA, ...))
-// of one box, or of one split-K chunk of a box, over the slots [s_begin, s_end).
+// One CTA of the mixed pass: the 128-row M tile `pair` (rows [128 pair,
+// 128 pair + 128)) of one box, or of one split-K chunk of a box, over the
+// slots [s_begin, s_end).
 struct MixItem {
   double cx, cy, cz;  // box centre
   double dk;          // mode spacing of the box's level
@@ -21,8 +22,11 @@ struct MixItem {
 
 // CTAs per box for n modes per axis half
 int mixed_pairs(int nk);
-// 2-D tensor map over the slot arrays x, y, z, q (stride slot_capacity, which must be even)
-void make_coord_map(CUtensorMap* map, const double* sx, int slot_capacity);
+// particles per pipeline chunk of the mixed pass for n modes per axis half
+int mixed_chunk(int nk);
+// 2-D tensor map over the slot arrays x, y, z, q (stride slot_capacity, which
+// must be even), in boxes of kcp + 2 slots
+void make_coord_map(CUtensorMap* map, const double* sx, int slot_capacity, int kcp);
 // max |q| over n charges into *out (one block)
 void launch_absmax(const double* sq, int n, double* out, cudaStream_t st);
 // one launch of the mixed pass over nitems device-resident items

@@ -1,6 +1,6 @@
 """Mixed precision (HPDMK_PRECISION_MIXED): the outgoing plane-wave
-expansions formed on the tensor cores (tcgen05 kind::i8) from three 8-bit
-slices (base 254) of each phase factor, against the oracle's FP64 expansions (the
+expansions formed on the tensor cores (tcgen05 kind::i8) from four signed
+8-bit slices (a 32-bit fixed point) of each phase-factor product, against the oracle's FP64 expansions (the
 reference's nudft3d1_halfplane, include/nudft.hpp:95-121, and the root pass,
 src/planewave.cpp:24-46); the energies and energy shifts that follow from
 them against the oracle and the FP64 Ewald energy."""
@@ -17,12 +17,13 @@ pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
-# Each slice product is exact (32-bit integer sums); an operand carries its
-# FP32 rounding and a slice truncation of at most 6e-8 of its range
-# (|factor| <= 1, charges scaled by max |q|), so a coefficient of a box of n
-# random-phase particles is off by about sqrt(n) 1e-7: the bound below is
-# relative to the largest coefficient of the box.
-REL_PW_MIXED = 1e-6
+# Each slice product is exact (32-bit integer sums); an operand carries the
+# rounding of its 32-bit fixed point (2.3e-10 of its range: |factor| <= 1,
+# charges scaled by max |q|) and the ten-product truncation (zero-mean, below
+# 1e-9 of the range), so a coefficient of a box of n random-phase particles
+# is off by about sqrt(n) 4e-10: the bound below is relative to the largest
+# coefficient of the box.
+REL_PW_MIXED = 2e-8
 ABS_DE_MIXED = 1e-8
 
 

@@ -2,11 +2,11 @@
 numpy on the same inputs the kernels see.
 
 1. The outgoing expansion of one box from 8-bit slices: the kernel's
-   arithmetic (FP32 phase factors, t = 127 v split as t = a1 + a2/254 +
-   a3/254^2, the six slice products summed exactly in integers, FP64
-   combination) against the FP64 direct NUDFT of the reference
-   (include/nudft.hpp:95-121). The coefficient error stays near the FP32
-   rounding of the operands.
+   arithmetic (FP64 phase factors, the 32-bit fixed point X = round(127 v
+   2^24) written as four signed base-256 digits, the ten slice products of
+   order s + t <= 5 summed exactly in integers, FP64 combination) against the FP64
+   direct NUDFT of the reference (include/nudft.hpp:95-121). The
+   coefficient error stays near 1e-9 of the largest coefficient.
 2. The near field in FP32 (box-centred coordinates, FP32 distance and the
    19-term residual polynomial in FP32) misses the 1e-8 energy target on the
    N = 1e5 cube, which is why the near field stays FP64 in both paths.
@@ -28,14 +28,12 @@ def f32(x):
 
 
 def slices(t):
-    """t (float32, |t| <= 127) -> int8 slices a1, a2, a3 with t ~ a1 + a2/254 + a3/254^2."""
-    t = t.astype(np.float64)
-    a1 = np.rint(t)
-    r1 = t - a1
-    a2 = np.rint(f32(r1 * 254.0).astype(np.float64))
-    r2 = f32(r1 * 254.0 - a2).astype(np.float64)
-    a3 = np.rint(f32(r2 * 254.0).astype(np.float64))
-    return [a.astype(np.int64) for a in (a1, a2, a3)]
+    """t (|t| <= 127) -> the signed base-256 digits of X = round(t 2^24),
+    highest first, t ~ sum_s a_s 256^-s, every a_s in [-128, 127]: the bytes
+    of X + 0x808080, the three lower ones less 128."""
+    Y = np.rint(t * 2.0 ** 24).astype(np.int64) + 0x808080
+    top = Y >> 24  # arithmetic shift: the signed top digit
+    return [top, ((Y >> 16) & 0xFF) - 128, ((Y >> 8) & 0xFF) - 128, (Y & 0xFF) - 128]
 
 
 def test_int8_slice_contraction_of_one_box():
@@ -52,33 +50,33 @@ def test_int8_slice_contraction_of_one_box():
     ez = np.exp(-1j * dk * np.outer(x[:, 2], mz)) * q[:, None]
     # FP64 reference: out[kz, ky, kx] = sum_j ez ey ex
     ref = np.einsum("jz,jy,jx->zyx", ez, ey, ex)
-    # the kernel: FP32 factors (ex scaled by 127, ez by 127 q / max|q|), A = ez ey in FP32
+    # the kernel: FP64 factors (ex scaled by 127, ez by 127 q / max|q|), A = ez ey in FP64
     qmax = np.abs(q).max()
-    exs = f32(127 * ex.real) + 1j * f32(127 * ex.imag)
-    eys = f32(ey.real) + 1j * f32(ey.imag)
-    ezs = f32(127 * ez.real / qmax) + 1j * f32(127 * ez.imag / qmax)
-    A = ezs[:, :, None] * eys[:, None, :]  # [j, kz, ky], products of FP32 values
-    Ar, Ai = f32(A.real), f32(A.imag)
-    Br, Bi = f32(exs.real), f32(exs.imag)
-    sa_r, sa_i, sb_r, sb_i = slices(Ar), slices(Ai), slices(Br), slices(Bi)
-    acc_re = [0, 0, 0]
-    acc_im = [0, 0, 0]
-    for s in range(3):
-        for t in range(3 - s):
+    A = (127 * ez / qmax)[:, :, None] * ey[:, None, :]  # [j, kz, ky]
+    B = 127 * ex
+    sa_r, sa_i, sb_r, sb_i = slices(A.real), slices(A.imag), slices(B.real), slices(B.imag)
+    acc_re = [0, 0, 0, 0]
+    acc_im = [0, 0, 0, 0]
+    for s in range(4):
+        for t in range(4 - s):
             # real output: Ar Br - Ai Bi; imaginary: Ar Bi + Ai Br (exact integers)
             acc_re[s + t] = acc_re[s + t] + np.einsum("jzy,jx->zyx", sa_r[s], sb_r[t]) - \
                 np.einsum("jzy,jx->zyx", sa_i[s], sb_i[t])
             acc_im[s + t] = acc_im[s + t] + np.einsum("jzy,jx->zyx", sa_r[s], sb_i[t]) + \
                 np.einsum("jzy,jx->zyx", sa_i[s], sb_r[t])
     scale = qmax / (127.0 * 127.0)
-    out = scale * ((acc_re[0] + acc_re[1] / 254.0 + acc_re[2] / 254.0 ** 2) +
-                   1j * (acc_im[0] + acc_im[1] / 254.0 + acc_im[2] / 254.0 ** 2))
+    w = [256.0 ** -k for k in range(4)]
+    out = scale * (sum(a * c for a, c in zip(acc_re, w)) + 1j * sum(a * c for a, c in zip(acc_im, w)))
+    # the digits are signed bytes, and the exact integer sums fit 32 bits for
+    # a split-K chunk of 8192 particles
+    assert all(np.abs(a).max() <= 128 for a in sa_r + sa_i + sb_r + sb_i)
+    assert max(np.abs(a).max() for a in acc_re + acc_im) * 8192 / n_box < 2 ** 31
     err = np.abs(out - ref).max() / np.abs(ref).max()
     rms = np.sqrt(np.mean(np.abs(out - ref) ** 2)) / np.sqrt(n_box)
     print(f"\nint8 slices, one box of {n_box}: max error {err:.2e} of the largest coefficient, "
           f"rms error per sqrt(particle) {rms:.2e}")
-    assert err < 1e-6
-    assert rms < 2e-7  # about the FP32 rounding of the operands
+    assert err < 2e-9
+    assert rms < 2e-9
 
 
 def test_fp32_near_field_misses_the_target():

@@ -96,6 +96,7 @@ def test_static_batch_allocates_nothing():
     # from) must not grow during the calls, not even transiently (its
     # high-water mark is reset first), and the device's free memory must not
     # change (plain allocations)
+    from cuda.bindings import driver as dr
     from cuda.bindings import runtime as rt
 
     def ok(res):
@@ -111,7 +112,7 @@ def test_static_batch_allocates_nothing():
         high_attr = rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh
         ok(rt.cudaDeviceSynchronize())
         used0 = int(ok(rt.cudaMemPoolGetAttribute(pool, used_attr)))
-        ok(rt.cudaMemPoolSetAttribute(pool, high_attr, rt.cuuint64_t(0)))  # reset to the current use
+        ok(rt.cudaMemPoolSetAttribute(pool, high_attr, dr.cuuint64_t(0)))  # reset to the current use
         free0, _ = ok(rt.cudaMemGetInfo())
         for m in (1, 64, P.STATIC_MAX_MOVES, 300):
             idx, disp = moves(rng, 3000, m, 0.4)
