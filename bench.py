@@ -46,9 +46,11 @@ WORKLOAD = dict(workload="uniform periodic cube, full energy + sequential Metrop
                          "mixed precision and FP64", N=1_000_000, L=100.0, digits=9, n_per_leaf=200,
                 moves_per_step=10000, candidates=4096, step=0.3, candidate_step=0.5, beta=1.0,
                 charges="alternating +1/-1")
+# 12 digits: at 9 the method's own error on this system is near 2e-8 of |E|,
+# above the 1e-8 target, so the precision is escalated
 CLUSTERED = dict(workload="64 isotropic Gaussian clusters (sigma = L/40) + 20 % uniform background", N=1_000_000,
-                 L=100.0, digits=9, n_per_leaf=200, moves_per_step=2000, step=0.3, beta=1.0,
-                 charges="alternating +1/-1")
+                 L=100.0, digits=12, digits_note="escalated from 9, whose error is near 2e-8 of |E| here",
+                 n_per_leaf=200, moves_per_step=2000, step=0.3, beta=1.0, charges="alternating +1/-1")
 WORKLOAD_N1E5 = dict(workload="uniform periodic cube, full energy + sequential Metropolis", N=100000, L=46.4,
                      digits=9, n_per_leaf=200, moves_per_step=10000, step=0.3, beta=1.0,
                      charges="alternating +1/-1")
@@ -350,20 +352,20 @@ class Arm:
         self.tree.close()
 
 
-def run_system(P, torch, W, r, q, args, ws, l2_flush, seed, cand, with_timing=False):
-    """FP64 and mixed arms on one system, alternating step by step; returns
-    (arms, launches in the timed region)."""
+def run_system(P, torch, W, r, q, args, ws, l2_flush, seed, cand, with_timing=False, names=("fp64", "mixed")):
+    """The FP64 and mixed arms (or those of `names`) on one system,
+    alternating step by step; returns (arms, launches in the timed region)."""
     M = W["moves_per_step"]
     nsteps = args.warmup + args.steps
-    arms = {"fp64": Arm(P, torch, W, r, q, P.PRECISION_FP64, M * nsteps, seed, cand),
-            "mixed": Arm(P, torch, W, r, q, P.PRECISION_MIXED, M * nsteps, seed, cand)}
+    prec = {"fp64": P.PRECISION_FP64, "mixed": P.PRECISION_MIXED}
+    arms = {k: Arm(P, torch, W, r, q, prec[k], M * nsteps, seed, cand) for k in names}
     launches = 0
     for s in range(nsteps):
         timed = s >= args.warmup
         if with_timing and s == args.warmup:
             arms["mixed"].tree.get_timing(reset=True)
             arms["mixed"].tree.set_timing(True)
-        for name in ("fp64", "mixed"):
+        for name in names:
             a = arms[name]
             barrier(ws)
             l0 = P.launch_count()
@@ -463,16 +465,19 @@ def run_b200(args, rank, ws):
     ew_cl = gpu_ewald(rc, qc, CLUSTERED)
     cargs = argparse.Namespace(**vars(args))
     cargs.steps = min(args.steps, 3)
-    carms, _ = run_system(P, torch, CLUSTERED, rc, qc, cargs, ws, l2_flush, seed=5 + rank, cand=0)
-    clustered = {k: a.summary(ws, ew_cl) for k, a in carms.items()}
+    # one arm at a time: at 12 digits a tree of this system holds about 50 GB
+    # of expansions
+    clustered = {}
+    for name in ("fp64", "mixed"):
+        carms, _ = run_system(P, torch, CLUSTERED, rc, qc, cargs, ws, l2_flush, seed=5 + rank, cand=0, names=(name,))
+        clustered[name] = carms[name].summary(ws, ew_cl)
+        carms[name].close()
+        del carms
+        torch.cuda.empty_cache()
     clustered["mixed_vs_fp64"] = {"full_energy": clustered["mixed"]["full_energy_evals_per_s"] /
                                   clustered["fp64"]["full_energy_evals_per_s"],
                                   "moves": clustered["mixed"]["moves_per_s"] / clustered["fp64"]["moves_per_s"]}
     clustered["config"] = dict(CLUSTERED, steps=cargs.steps)
-    for a in carms.values():
-        a.close()
-    del carms
-    torch.cuda.empty_cache()
 
     # the N = 1e5 cube, against the stored CPU Ewald energy
     W5 = dict(WORKLOAD_N1E5)

@@ -981,6 +981,23 @@ void DmkTree::form_outgoing_pw() {
     k_reduce_chunks<<<grid, TPB, 0, st>>>(pbase, d_meta, d_meta + nbx, d_outs, H);
     PDMK_LAUNCH_CHECK();
   };
+  // the mixed pass's chunk tables: one block of mixed_table_bytes per chunk
+  // of each slot range, shared by the range's consecutive tile items; the
+  // chunk list names each chunk's range by its first tile item
+  auto plan_mix_tables = [&](int nk, std::vector<MixItem>& wl, unsigned char** tab, std::vector<int2>& ch) {
+    const int kcp = mixed_chunk(nk), tiles = mixed_pairs(nk);
+    const size_t tb = size_t(mixed_table_bytes(nk));
+    size_t total = 0;
+    for (size_t i = 0; i < wl.size(); i += tiles) total += size_t((wl[i].s_end - wl[i].s_begin + kcp - 1) / kcp);
+    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(tab), total * tb + 16, st_));
+    size_t cur = 0;
+    for (size_t i = 0; i < wl.size(); i += tiles) {
+      const int n = (wl[i].s_end - wl[i].s_begin + kcp - 1) / kcp;
+      for (int t = 0; t < tiles; ++t) wl[i + t].tab = *tab + cur * tb;
+      for (int c = 0; c < n; ++c) ch.push_back(make_int2(int(i), c));
+      cur += size_t(n);
+    }
+  };
   if (!aux_) {
     PDMK_CUDA(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking));
     PDMK_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
@@ -1003,10 +1020,12 @@ void DmkTree::form_outgoing_pw() {
     else make_work(wroot, D.n_window, 0, 0, part_r + size_t(c) * D.Hw, sb, se);
   }
   double2* tab_root = nullptr;
+  unsigned char* mtab_root = nullptr;
   std::vector<int2> ch_root;
   size_t rch, rmeta, rout;
   unsigned char* d_root = nullptr;
   if (mixed) {
+    plan_mix_tables(D.n_window, mroot, &mtab_root, ch_root);
     d_root = upload(mroot, ch_root, root_split, &rch, &rmeta, &rout);
   } else {
     plan_nudft_tables(D.n_window, wroot, &tab_root, ch_root, st_);
@@ -1015,8 +1034,8 @@ void DmkTree::form_outgoing_pw() {
   PDMK_CUDA(cudaEventRecord(ev_fork_, st_));
   PDMK_CUDA(cudaStreamWaitEvent(aux_, ev_fork_, 0));
   if (mixed)
-    dispatch_mixed(D.n_window, tmap_root, reinterpret_cast<const MixItem*>(d_root), int(mroot.size()), d_mix_, d_mix_err,
-                   aux_);
+    dispatch_mixed(D.n_window, tmap_root, reinterpret_cast<const MixItem*>(d_root), int(mroot.size()),
+                   reinterpret_cast<const int2*>(d_root + rch), int(ch_root.size()), d_mix_, d_mix_err, aux_);
   else
     dispatch_nudft(D.n_window, reinterpret_cast<const NudftWork*>(d_root), int(wroot.size()),
                    reinterpret_cast<const int2*>(d_root + rch), int(ch_root.size()), D, aux_);
@@ -1091,10 +1110,12 @@ void DmkTree::form_outgoing_pw() {
     }
   }
   double2* tab_box = nullptr;
+  unsigned char* mtab_box = nullptr;
   std::vector<int2> ch_box;
   size_t bch, bmeta, bout;
   unsigned char* d_box = nullptr;
   if (mixed) {
+    plan_mix_tables(D.n_diff, mbox, &mtab_box, ch_box);
     d_box = upload(mbox, ch_box, box_split, &bch, &bmeta, &bout);
   } else {
     plan_nudft_tables(D.n_diff, wbox, &tab_box, ch_box, st_);
@@ -1102,8 +1123,8 @@ void DmkTree::form_outgoing_pw() {
   }
   time_begin(3);
   if (mixed)
-    dispatch_mixed(D.n_diff, tmap_box, reinterpret_cast<const MixItem*>(d_box), int(mbox.size()), d_mix_, d_mix_err,
-                   st_);
+    dispatch_mixed(D.n_diff, tmap_box, reinterpret_cast<const MixItem*>(d_box), int(mbox.size()),
+                   reinterpret_cast<const int2*>(d_box + bch), int(ch_box.size()), d_mix_, d_mix_err, st_);
   else
     dispatch_nudft(D.n_diff, reinterpret_cast<const NudftWork*>(d_box), int(wbox.size()),
                    reinterpret_cast<const int2*>(d_box + bch), int(ch_box.size()), D, st_);
@@ -1111,8 +1132,9 @@ void DmkTree::form_outgoing_pw() {
   reduce(box_split, part_b, D.H, d_box, bmeta, bout, st_);
   // the root pass's buffers are released after it joins the tree's stream
   PDMK_CUDA(cudaStreamWaitEvent(st_, ev_join_, 0));
-  for (void* p : {static_cast<void*>(d_root), static_cast<void*>(tab_root), static_cast<void*>(part_r),
-                  static_cast<void*>(d_box), static_cast<void*>(tab_box), static_cast<void*>(part_b)})
+  for (void* p : {static_cast<void*>(d_root), static_cast<void*>(tab_root), static_cast<void*>(mtab_root),
+                  static_cast<void*>(part_r), static_cast<void*>(d_box), static_cast<void*>(tab_box),
+                  static_cast<void*>(mtab_box), static_cast<void*>(part_b)})
     if (p) PDMK_CUDA(cudaFreeAsync(p, st_));
   diff_cached_ = false;
 }

@@ -32,21 +32,24 @@
 // Yokota (DGEMM on integer matrix multiplication units, 2024), applied to
 // operands bounded by one.
 //
-// One CTA computes one 128-row M tile of one box (or split-K chunk of a box)
-// and streams the box's particles through shared memory KCP at a time:
-//   - producer warps: TMA (cp.async.bulk.tensor) brings the next chunk's
-//     coordinates and charges into shared memory; the chunk's phase factors
-//     are formed in FP64 (box-centred phases, exact sixth roots of unity for
-//     the decentring; one task per particle, axis and half of the mode
-//     range), and the B operand is sliced;
-//   - consumer warps: one output row (kz, ky) per thread forms A = ez ey in
-//     FP64 and slices it;
-//   - one consumer thread issues the MMAs and commits them to an mbarrier;
-//     the shared-memory stages are double-buffered, so the tensor core works
-//     on chunk c while the warps build chunk c + 1;
-//   - epilogue: tcgen05.ld of the accumulators, FP64 combination, staging
-//     in shared memory and one bulk copy (cp.async.bulk) into the box's
-//     expansion row range, which is contiguous in HBM.
+// Two kernels per pass:
+//   - k_pw_tables, one CTA per 32-particle chunk of a box: TMA
+//     (cp.async.bulk.tensor) brings the chunk's coordinates and charges into
+//     shared memory; the phase factors are formed in FP64 (box-centred
+//     phases, exact sixth roots of unity for the decentring; one thread per
+//     particle, axis and half of the mode range), the B operand is sliced
+//     into the tensor core's shared-memory layout, and the block (B slices,
+//     ey and ez factors) goes to HBM with one bulk copy. Every M tile of the
+//     box reads these once-formed tables.
+//   - k_pw_mixed, one CTA per 128-row M tile of a box (or split-K chunk): a
+//     control warp brings each chunk's table block into shared memory with a
+//     bulk copy (three chunks in flight) and issues the MMAs; the consumer
+//     warps form A = ez ey in FP64, one thread per output row (kz, ky) and
+//     group of 8 particles, and slice it; the A stages are double-buffered, so the tensor
+//     core works on chunk c while the consumers build chunk c + 1; the
+//     epilogue reads the accumulators (tcgen05.ld), combines them in FP64,
+//     stages the rows in shared memory and writes them with one bulk copy
+//     into the box's expansion row range, which is contiguous in HBM.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -64,59 +67,70 @@
 namespace pdmk {
 namespace {
 
-constexpr int RPC = 128;  // rows (one M tile) per CTA, one consumer thread each
-constexpr int NACC = 4;   // accumulators: slice-product orders s + t = 2 .. 5
+constexpr int RPC = 128;           // rows (one M tile) per CTA
+constexpr int NACC = 4;            // accumulators: slice-product orders s + t = 2 .. 5
+constexpr int TSTAGES = 3;         // table blocks in flight per CTA
 
-// smem footprint of the pipeline for a chunk of kcp particles
-__host__ __device__ constexpr int mix_pipe_bytes(int nk, int kcp) {
-  return 2 * 4 * RPC * 2 * kcp                          // A stages: 4 slices x rows x K bytes
-         + 2 * 4 * ((2 * (2 * nk + 1) + 15) / 16 * 16) * 2 * kcp  // B stages
-         + 2 * kcp * (2 * (2 * nk + 1) + nk + 1) * 16    // FP64 factor stages (ex, ey, ez)
-         + 2 * (((4 * (kcp + 2) * 8) + 127) / 128 * 128) // coordinate stages
-         + 1024;                                         // alignment slack
+__host__ __device__ constexpr int npad_of(int nk) { return (2 * (2 * nk + 1) + 15) / 16 * 16; }
+__host__ __device__ constexpr int ezs_of(int nk) { return (nk + 1) | 1; }
+// bytes of one chunk's table block: B slices, then the ey and ez factors
+__host__ __device__ constexpr int table_bytes(int nk, int kcp) {
+  return 4 * npad_of(nk) * 2 * kcp + kcp * ((2 * nk + 1) + ezs_of(nk)) * 16;
+}
+// shared memory of the contraction kernel for chunks of kcp particles
+__host__ __device__ constexpr int mix_smem_bytes(int nk, int kcp) {
+  return 2 * 4 * RPC * 2 * kcp + TSTAGES * ((table_bytes(nk, kcp) + 127) / 128 * 128) + 1024;
 }
 
 template <int NK>
 struct MixShape {
   static constexpr int D = 2 * NK + 1;
   static constexpr int ROWS = (NK + 1) * D;
-  static constexpr int NPAD = (2 * D + 15) / 16 * 16;  // MMA N: Re columns [0, D), Im columns [HALF, HALF + D)
+  static constexpr int NPAD = npad_of(NK);  // MMA N: Re columns [0, D), Im columns [HALF, HALF + D)
   static constexpr int HALF = NPAD / 2;
+  static constexpr int EZS = ezs_of(NK);    // odd row strides keep 16-byte stores on distinct bank groups
   static constexpr int TILES = (ROWS + RPC - 1) / RPC;  // CTAs per box
   // particles per chunk: 32 when the stages fit, else 16
-  static constexpr int KCP = mix_pipe_bytes(NK, 32) <= 227 * 1024 ? 32 : 16;
-  static constexpr int KB = 2 * KCP;                    // K bytes per chunk (real and imaginary part per particle)
-  static constexpr int KSTEPS = KB / 32;                // MMA K steps (32 bytes each) per chunk
-  static constexpr int PTHREADS = 6 * KCP;              // producers: one task per (particle, axis, half)
-  static constexpr int THREADS = RPC + PTHREADS;
-  static constexpr int COORD_BOX = KCP + 2;             // TMA box along the slots: even start, one spare each side
+  static constexpr int KCP = mix_smem_bytes(NK, 32) <= 227 * 1024 ? 32 : 16;
+  static constexpr int KB = 2 * KCP;        // K bytes per chunk (real and imaginary part per particle)
+  static constexpr int KSTEPS = KB / 32;    // MMA K steps (32 bytes each) per chunk
+  static constexpr int CPR = KB / 16;            // consumer threads per row: one per 16-byte K group (8 particles)
+  static constexpr int CTHREADS = RPC * CPR;
+  static constexpr int THREADS = CTHREADS + 32;  // consumers + the control warp
+  static constexpr int TTHREADS = 6 * KCP;       // table kernel: one thread per (particle, axis, half)
+  static constexpr int COORD_BOX = KCP + 2;      // TMA box along the slots: even start, one spare each side
   static constexpr int COORD_BYTES = 4 * COORD_BOX * 8;
-  static constexpr int COORD_STRIDE = (COORD_BYTES + 127) / 128 * 128;
   static constexpr int TCOLS_USED = NACC * NPAD;
   static constexpr int TCOLS = TCOLS_USED <= 32 ? 32 : TCOLS_USED <= 64 ? 64 : TCOLS_USED <= 128 ? 128
                                : TCOLS_USED <= 256 ? 256 : 512;
-  // shared memory (bytes)
-  static constexpr int A_SLICE = RPC * KB;
+  // one chunk's table block
   static constexpr int B_SLICE = NPAD * KB;
+  static constexpr int B_BYTES = 4 * B_SLICE;
+  static constexpr int EY_OFF = B_BYTES;
+  static constexpr int EZ_OFF = EY_OFF + KCP * D * 16;
+  static constexpr int T_BYTES = EZ_OFF + KCP * EZS * 16;
+  static constexpr int T_STRIDE = (T_BYTES + 127) / 128 * 128;
+  // contraction kernel shared memory
+  static constexpr int A_SLICE = RPC * KB;
   static constexpr int A_STAGE = 4 * A_SLICE;
-  static constexpr int B_STAGE = 4 * B_SLICE;
-  static constexpr int F_STAGE = KCP * (2 * D + NK + 1) * 16;  // ex, ey, ez as double2
   static constexpr int OFF_A = 0;
-  static constexpr int OFF_B = OFF_A + 2 * A_STAGE;
-  static constexpr int OFF_F = OFF_B + 2 * B_STAGE;
-  static constexpr int OFF_P = (OFF_F + 2 * F_STAGE + 127) / 128 * 128;
-  static constexpr int PIPE_BYTES = OFF_P + 2 * COORD_STRIDE;
+  static constexpr int OFF_T = OFF_A + 2 * A_STAGE;
+  static constexpr int PIPE_BYTES = OFF_T + TSTAGES * T_STRIDE;
   static constexpr int STAGE_OUT = RPC * D * 16;  // epilogue staging, reuses the pipeline buffers
   static constexpr int SMEM = (PIPE_BYTES > STAGE_OUT ? PIPE_BYTES : STAGE_OUT) + 1024;  // + alignment slack
+  // table kernel shared memory: coordinates, ex scratch, the block
+  static constexpr int TK_OFF_EX = (COORD_BYTES + 127) / 128 * 128;
+  static constexpr int TK_OFF_T = (TK_OFF_EX + KCP * D * 16 + 127) / 128 * 128;
+  static constexpr int TK_SMEM = TK_OFF_T + T_STRIDE + 1024;
   static_assert(TCOLS_USED <= 512, "accumulators exceed TMEM");
   static_assert(HALF >= D, "imaginary columns overlap the real ones");
-  static_assert(SMEM <= 227 * 1024, "shared memory");
+  static_assert(SMEM <= 227 * 1024 && TK_SMEM <= 227 * 1024, "shared memory");
   static_assert(KB % 32 == 0, "chunks are whole MMA K steps");
-  static_assert(PTHREADS % 32 == 0, "producer warps");
+  static_assert(T_BYTES % 16 == 0, "bulk copies move multiples of 16 bytes");
 };
 
-// named barrier ids
-constexpr int BAR_FULL0 = 1, BAR_EMPTY0 = 3, BAR_CONS = 5, BAR_PROD = 6;
+// named barrier ids: A stage s ready (consumers -> control), consumers only
+constexpr int BAR_AREADY0 = 1, BAR_CONS = 5;
 
 constexpr double SL_SCALE = 127.0;  // operands are scaled to |t| <= 127
 
@@ -168,16 +182,61 @@ __device__ __forceinline__ double2 root6_d(int m) {
   }
 }
 
+// sin and cos of th, |th| <= pi (slots hold particles inside their box, or
+// the leaf centre when empty, so th = dk (x - c) stays in range: |th| <= pi / 3
+// at the difference levels, <= pi at the root): the Taylor series of sin and
+// cos at h = th / 2 (|h| <= pi / 2; the first omitted terms are below 1e-19)
+// as two Horner chains in h^2, then the double-angle formulas
+__device__ __forceinline__ void sincos_taylor(double th, double& s, double& c) {
+  const double h = 0.5 * th, h2 = h * h;
+  double ps = 6.446950284384474e-26, pc = 1.6117375710961184e-24;
+  ps = fma(ps, h2, -3.868170170630684e-23);
+  pc = fma(pc, h2, -8.896791392450574e-22);
+  ps = fma(ps, h2, 1.9572941063391263e-20);
+  pc = fma(pc, h2, 4.110317623312165e-19);
+  ps = fma(ps, h2, -8.22063524662433e-18);
+  pc = fma(pc, h2, -1.5619206968586225e-16);
+  ps = fma(ps, h2, 2.8114572543455206e-15);
+  pc = fma(pc, h2, 4.779477332387385e-14);
+  ps = fma(ps, h2, -7.647163731819816e-13);
+  pc = fma(pc, h2, -1.1470745597729725e-11);
+  ps = fma(ps, h2, 1.6059043836821613e-10);
+  pc = fma(pc, h2, 2.08767569878681e-09);
+  ps = fma(ps, h2, -2.505210838544172e-08);
+  pc = fma(pc, h2, -2.755731922398589e-07);
+  ps = fma(ps, h2, 2.7557319223985893e-06);
+  pc = fma(pc, h2, 2.48015873015873e-05);
+  ps = fma(ps, h2, -0.0001984126984126984);
+  pc = fma(pc, h2, -0.001388888888888889);
+  ps = fma(ps, h2, 0.008333333333333333);
+  pc = fma(pc, h2, 0.041666666666666664);
+  ps = fma(ps, h2, -0.16666666666666666);
+  pc = fma(pc, h2, -0.5);
+  ps = fma(ps, h2, 1.0);
+  pc = fma(pc, h2, 1.0);
+  const double sh = ps * h;  // sin(h)
+  s = 2.0 * sh * pc;         // sin(2h) = 2 sin(h) cos(h)
+  c = fma(-2.0 * sh, sh, 1.0);  // cos(2h) = 1 - 2 sin(h)^2
+}
+
 // FP64 phase factors exp(-i m dk (x - c)) w6^{-M (2X+1) m} for m = m0 .. m0 + cnt - 1,
-// times `scale`, into dst[0 .. cnt) (six interleaved recurrence chains, each
-// with its own exact root of unity, as in the FP64 path)
+// times `scale`, into dst[0 .. cnt): the step exp(-i th), the start
+// exp(-i m0 th) by binary powering of the step (|m0| <= 26: at most five
+// squarings), then six interleaved recurrence chains, each with its own
+// exact root of unity, as in the FP64 path
 __device__ void axis_factors_d(double xr, double dk, int M, int X, int m0, int cnt, double scale, double2* dst) {
   const double th = dk * xr;
   double s, c;
-  sincos(-double(m0) * th, &s, &c);
-  const double2 v0 = make_double2(c * scale, s * scale);
-  sincos(-th, &s, &c);
+  sincos_taylor(-th, s, c);
   const double2 st = make_double2(c, s);
+  double2 v0 = make_double2(scale, 0.0);
+  {
+    double2 w = m0 < 0 ? make_double2(c, -s) : st;  // exp(+i th) for negative powers
+    for (int e = m0 < 0 ? -m0 : m0; e; e >>= 1) {
+      if (e & 1) v0 = cmul_d(v0, w);
+      w = cmul_d(w, w);
+    }
+  }
   const double2 st2 = cmul_d(st, st), st3 = cmul_d(st2, st), st6 = cmul_d(st3, st3);
   const int dec = M * (2 * X + 1);
   double2 v[6];
@@ -202,36 +261,127 @@ __device__ void axis_factors_d(double xr, double dk, int M, int X, int m0, int c
 
 
 
+// Table pass: the FP64 phase factors of one chunk of one box, the sliced B
+// operand in the tensor core's K-major layout ([slice][16-byte K group][column]
+// [16 bytes]) and the ey, ez factors ([particle][mode], double2), written to
+// the chunk's table block. One thread per (particle, axis, half of the mode
+// range), consecutive lanes on consecutive particles.
 template <int NK>
-__global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
-    k_pw_mixed(const __grid_constant__ CUtensorMap coords, const MixItem* __restrict__ items,
-               const double* __restrict__ qmax_p, int* __restrict__ err) {
+__global__ void __launch_bounds__(MixShape<NK>::TTHREADS)
+    k_pw_tables(const __grid_constant__ CUtensorMap coords, const MixItem* __restrict__ items,
+                const int2* __restrict__ chunks, const double* __restrict__ qmax_p, int* __restrict__ err) {
   using S = MixShape<NK>;
   constexpr int D = S::D, NPAD = S::NPAD, HALF = S::HALF, KCP = S::KCP, KB = S::KB;
   extern __shared__ unsigned char smem_raw[];
-  unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // the 1024-aligned base as an offset from the shared array, so that the
+  // compiler keeps shared-memory (not generic) loads and stores
+  unsigned char* sm = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
+  __shared__ __align__(8) uint64_t bar;
+  const int tid = threadIdx.x;
+  const int2 ch = chunks[blockIdx.x];
+  const MixItem it = items[ch.x];
+  const int sb = it.s_begin + ch.y * KCP;
+  const int nk = min(KCP, it.s_end - sb);
+  const int off = sb - (sb & ~1);
+  const double qmax = *qmax_p;
+  const double inv_qmax = qmax > 0.0 ? 1.0 / qmax : 0.0;
+  const double* P = reinterpret_cast<const double*>(sm);
+  double2* ex = reinterpret_cast<double2*>(sm + S::TK_OFF_EX);
+  unsigned char* blk = sm + S::TK_OFF_T;
+  double2* ey = reinterpret_cast<double2*>(blk + S::EY_OFF);
+  double2* ez = reinterpret_cast<double2*>(blk + S::EZ_OFF);
+  if (tid == 0) {
+    tc::mbar_init(&bar, 1);
+    tc::mbar_fence_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    tc::mbar_arrive_expect_tx(&bar, S::COORD_BYTES);
+    tc::tma_load_2d(sm, &coords, sb & ~1, 0, &bar);
+  }
+  if (!tc::mbar_wait(&bar, 0)) atomicOr(err, 4);  // bounded; the zero-filled buffer is then still read safely
+  {
+    const int j = tid % KCP, ah = tid / KCP, a = ah >> 1, half = ah & 1;
+    const int len = a == 2 ? NK + 1 : D;
+    const int h0 = (len + 1) / 2;
+    const int m0 = half ? -NK + h0 : -NK, cnt = half ? len - h0 : h0;
+    double2* dst = (a == 0 ? ex + j * D : (a == 1 ? ey + j * D : ez + j * S::EZS)) + (m0 + NK);
+    if (j < nk) {
+      const double xa = P[a * S::COORD_BOX + off + j];
+      const double ca = a == 0 ? it.cx : (a == 1 ? it.cy : it.cz);
+      const int Xa = a == 0 ? it.X : (a == 1 ? it.Y : it.Z);
+      const double scale = a == 0 ? SL_SCALE : (a == 1 ? 1.0 : SL_SCALE * P[3 * S::COORD_BOX + off + j] * inv_qmax);
+      axis_factors_d(xa - ca, it.dk, it.M, Xa, m0, cnt, scale, dst);
+    } else {
+      for (int m = 0; m < cnt; ++m) dst[m] = make_double2(0.0, 0.0);
+    }
+  }
+  __syncthreads();
+  // B operand from ex: column n < D is the real part of mode kx = n, column
+  // HALF + kx its imaginary part; K rows (2j, 2j+1) carry (Br, -Bi) for a
+  // real column and (Bi, Br) for an imaginary one
+  const uint32_t bbase = tc::smem_u32(blk);
+  for (int task = tid; task < NPAD * (KB / 16); task += S::TTHREADS) {
+    const int n = task % NPAD, kc = task / NPAD;
+    uint32_t w[4][4];
+    const bool re = n < D, im = n >= HALF && n < HALF + D;
+    const int kx = re ? n : n - HALF;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const int j0 = kc * 8 + 2 * p;
+      double2 v0 = make_double2(0.0, 0.0), v1 = make_double2(0.0, 0.0);
+      if (re || im) {
+        const double2 e0 = ex[j0 * D + kx], e1 = ex[(j0 + 1) * D + kx];
+        v0 = re ? make_double2(e0.x, -e0.y) : make_double2(e0.y, e0.x);
+        v1 = re ? make_double2(e1.x, -e1.y) : make_double2(e1.y, e1.x);
+      }
+      uint32_t by[4];
+      transpose4(fix24(v0.x), fix24(v0.y), fix24(v1.x), fix24(v1.y), by);
+#pragma unroll
+      for (int sl = 0; sl < 4; ++sl) w[sl][p] = by[3 - sl];  // slice 0 = the top byte
+    }
+#pragma unroll
+    for (int sl = 0; sl < 4; ++sl)
+      st_shared_v4(bbase + sl * S::B_SLICE + kc * (NPAD * 16) + n * 16, w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
+  }
+  tc::fence_async_smem();
+  __syncthreads();
+  if (tid == 0) {
+    tc::bulk_store(const_cast<unsigned char*>(it.tab) + size_t(ch.y) * S::T_BYTES, blk, S::T_BYTES);
+    tc::bulk_commit();
+    tc::bulk_wait_all();
+  }
+}
+
+// Contraction: one 128-row M tile of one box (or split-K chunk) over its
+// chunks' table blocks.
+template <int NK>
+__global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
+    k_pw_mixed(const MixItem* __restrict__ items, const double* __restrict__ qmax_p, int* __restrict__ err) {
+  using S = MixShape<NK>;
+  constexpr int D = S::D, NPAD = S::NPAD, HALF = S::HALF, KCP = S::KCP;
+  extern __shared__ unsigned char smem_raw[];
+  // the 1024-aligned base as an offset from the shared array, so that the
+  // compiler keeps shared-memory (not generic) loads and stores
+  unsigned char* sm = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
   __shared__ __align__(8) uint64_t mma_bar[2];
-  __shared__ __align__(8) uint64_t tma_bar[2];
+  __shared__ __align__(8) uint64_t tma_bar[TSTAGES];
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
-  const bool producer = tid >= RPC;
-  const int ptid = tid - RPC;
+  const bool control = tid >= S::CTHREADS;
   const MixItem it = items[blockIdx.x];
   const int row0 = it.pair * RPC;
   const int nrows = min(RPC, S::ROWS - row0);  // valid rows of this CTA
-  const int ntot = it.s_end - it.s_begin;
-  const int nch = (ntot + KCP - 1) / KCP;
+  const int nch = (it.s_end - it.s_begin + KCP - 1) / KCP;
   const double qmax = *qmax_p;
-  const double inv_qmax = qmax > 0.0 ? 1.0 / qmax : 0.0;
 
   if (tid == 0) {
     tc::mbar_init(&mma_bar[0], 1);
     tc::mbar_init(&mma_bar[1], 1);
-    tc::mbar_init(&tma_bar[0], 1);
-    tc::mbar_init(&tma_bar[1], 1);
+    for (int i = 0; i < TSTAGES; ++i) tc::mbar_init(&tma_bar[i], 1);
     tc::mbar_fence_init();
     s_abort = 0;
   }
@@ -248,109 +398,83 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
       s_abort = 1;
     }
   };
-  int last_tma = -1;     // the last chunk whose coordinates were requested (producer thread 0)
-  int last_commit = -1;  // the last chunk whose MMAs were committed (consumer thread 0)
+  auto fetch = [&](int c) {  // chunk c's table block into table stage c % TSTAGES
+    const int t = c % TSTAGES;
+    tc::mbar_arrive_expect_tx(&tma_bar[t], S::T_BYTES);
+    tc::bulk_load(sm + S::OFF_T + t * S::T_STRIDE, it.tab + size_t(c) * S::T_BYTES, S::T_BYTES, &tma_bar[t]);
+  };
+  int last_fetch = -1;   // the last chunk requested (control lane 0)
+  int last_commit = -1;  // the last chunk whose MMAs were committed (control lane 0)
 
-  if (producer) {
-    // ------------------------------------------------------------ producers
-    if (ptid == 0 && nch > 0) {
-      tc::tma_prefetch_desc(&coords);
-      tc::mbar_arrive_expect_tx(&tma_bar[0], S::COORD_BYTES);
-      tc::tma_load_2d(sm + S::OFF_P, &coords, it.s_begin & ~1, 0, &tma_bar[0]);
-      last_tma = 0;
-    }
+  if (control) {
+    // ------------------------------------------------------------ control warp
+    const bool lead = (tid & 31) == 0;
+    if (lead)
+      for (int c = 0; c < min(TSTAGES, nch); ++c) {
+        fetch(c);
+        last_fetch = c;
+      }
     for (int c = 0; c < nch; ++c) {
-      const int s = c & 1;
-      const uint32_t u = uint32_t(c >> 1);
-      if (c >= 2) tc::bar_sync(BAR_EMPTY0 + s, S::THREADS);
-      wait_bar(&tma_bar[s], u & 1);
-      const int sb = it.s_begin + c * KCP;
-      const int nk = min(KCP, it.s_end - sb);
-      const int off = sb - (sb & ~1);
-      const double* P = reinterpret_cast<const double*>(sm + S::OFF_P + s * S::COORD_STRIDE);
-      double2* ex = reinterpret_cast<double2*>(sm + S::OFF_F + s * S::F_STAGE);
-      double2* ey = ex + KCP * D;
-      double2* ez = ey + KCP * D;
-      {
-        // phase factors: one task per (particle, axis, half of the mode range)
-        const int j = ptid / 6, a = (ptid >> 1) % 3, half = ptid & 1;
-        const int len = a == 2 ? NK + 1 : D;
-        const int h0 = (len + 1) / 2;
-        const int m0 = half ? -NK + h0 : -NK, cnt = half ? len - h0 : h0;
-        double2* dst = (a == 0 ? ex + j * D : (a == 1 ? ey + j * D : ez + j * (NK + 1))) + (m0 + NK);
-        if (j < nk) {
-          const double xa = P[a * S::COORD_BOX + off + j];
-          const double ca = a == 0 ? it.cx : (a == 1 ? it.cy : it.cz);
-          const int Xa = a == 0 ? it.X : (a == 1 ? it.Y : it.Z);
-          const double scale =
-              a == 0 ? SL_SCALE : (a == 1 ? 1.0 : SL_SCALE * P[3 * S::COORD_BOX + off + j] * inv_qmax);
-          axis_factors_d(xa - ca, it.dk, it.M, Xa, m0, cnt, scale, dst);
-        } else {
-          for (int m = 0; m < cnt; ++m) dst[m] = make_double2(0.0, 0.0);
-        }
-      }
-      tc::bar_sync(BAR_PROD, S::PTHREADS);
-      // the next chunk's coordinates: its buffer was last read before the
-      // previous producer barrier
-      if (ptid == 0 && c + 1 < nch && !s_abort) {
-        tc::mbar_arrive_expect_tx(&tma_bar[s ^ 1], S::COORD_BYTES);
-        tc::tma_load_2d(sm + S::OFF_P + (s ^ 1) * S::COORD_STRIDE, &coords, (it.s_begin + (c + 1) * KCP) & ~1, 0,
-                        &tma_bar[s ^ 1]);
-        last_tma = c + 1;
-      }
-      // B operand: the MMAs of chunk c - 2 must have finished reading it
-      if (c >= 2) wait_bar(&mma_bar[s], (u - 1) & 1);
-      const uint32_t bbase = tc::smem_u32(sm + S::OFF_B + s * S::B_STAGE);
-      for (int task = ptid; task < NPAD * (KB / 16); task += S::PTHREADS) {
-        const int n = task % NPAD, kc = task / NPAD;
-        uint32_t w[4][4];
-        const bool re = n < D, im = n >= HALF && n < HALF + D;
-        const int kx = re ? n : n - HALF;
+      const int s2 = c & 1, t = c % TSTAGES;
+      tc::bar_sync(BAR_AREADY0 + s2, S::THREADS);  // A of chunk c is in shared memory (and its tables landed)
+      if (lead && !s_abort) {
+        tc::tc_fence_after();
+        const uint32_t abase = tc::smem_u32(sm + S::OFF_A + s2 * S::A_STAGE);
+        const uint32_t bbase = tc::smem_u32(sm + S::OFF_T + t * S::T_STRIDE);
+        constexpr uint32_t LBO_A = RPC * 16, LBO_B = NPAD * 16;
 #pragma unroll
-        for (int p = 0; p < 4; ++p) {
-          const int j0 = kc * 8 + 2 * p;
-          double2 v0 = make_double2(0.0, 0.0), v1 = make_double2(0.0, 0.0);
-          if (re || im) {
-            const double2 e0 = ex[j0 * D + kx], e1 = ex[(j0 + 1) * D + kx];
-            // K rows (2j, 2j+1) of a real output column: (Br, -Bi); of an imaginary one: (Bi, Br)
-            v0 = re ? make_double2(e0.x, -e0.y) : make_double2(e0.y, e0.x);
-            v1 = re ? make_double2(e1.x, -e1.y) : make_double2(e1.y, e1.x);
+        for (int ks = 0; ks < S::KSTEPS; ++ks) {
+          const uint32_t ka = abase + ks * 2 * LBO_A;
+          const uint32_t kb = bbase + ks * 2 * LBO_B;
+          // slice products (a slice sa, b slice sb) of order sa + sb <= 3, into accumulator sa + sb
+#pragma unroll
+          for (int sa = 0; sa < 4; ++sa) {
+#pragma unroll
+            for (int sb = 0; sb + sa < 4; ++sb) {
+              const uint32_t first = (c == 0 && ks == 0 && sa == 0) ? 0u : 1u;
+              tc::mma_i8(tmem + uint32_t((sa + sb) * NPAD), tc::smem_desc(ka + sa * S::A_SLICE, LBO_A, 128),
+                         tc::smem_desc(kb + sb * S::B_SLICE, LBO_B, 128), tc::idesc_i8(RPC, NPAD), first);
+            }
           }
-          uint32_t by[4];
-          transpose4(fix24(v0.x), fix24(v0.y), fix24(v1.x), fix24(v1.y), by);
-#pragma unroll
-          for (int sl = 0; sl < 4; ++sl) w[sl][p] = by[3 - sl];  // slice 0 = the top byte
         }
-#pragma unroll
-        for (int sl = 0; sl < 4; ++sl)
-          st_shared_v4(bbase + sl * S::B_SLICE + kc * (NPAD * 16) + n * 16, w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
+        tc::mma_commit(&mma_bar[s2]);
+        last_commit = c;
+        // the table stage of chunk c is free once these MMAs have read its B
+        // (the consumers are past its factors: they signalled above)
+        if (c + TSTAGES < nch) {
+          wait_bar(&mma_bar[s2], uint32_t(c >> 1) & 1);
+          if (!s_abort) {
+            fetch(c + TSTAGES);
+            last_fetch = c + TSTAGES;
+          }
+        }
       }
-      tc::fence_async_smem();
-      tc::bar_arrive(BAR_FULL0 + s, S::THREADS);
+      __syncwarp();
     }
   } else {
     // ------------------------------------------------------------ consumers
-    const int lr = tid;  // local row
+    const int lr = tid & (RPC - 1);  // local row
+    const int kh = tid / RPC;        // this thread's 16-byte K group (8 particles) of each chunk
     const int r = row0 + lr;
     const bool active = lr < nrows;
     const int kz = active ? r / D : 0, ky = active ? r % D : 0;
     for (int c = 0; c < nch; ++c) {
-      const int s = c & 1;
-      const uint32_t u = uint32_t(c >> 1);
-      tc::bar_sync(BAR_FULL0 + s, S::THREADS);
-      if (c >= 2) wait_bar(&mma_bar[s], (u - 1) & 1);
-      const uint32_t abase = tc::smem_u32(sm + S::OFF_A + s * S::A_STAGE);
+      const int s2 = c & 1, t = c % TSTAGES;
+      wait_bar(&tma_bar[t], uint32_t(c / TSTAGES) & 1);    // this chunk's tables have landed
+      if (c >= 2) wait_bar(&mma_bar[s2], uint32_t((c >> 1) - 1) & 1);  // A stage s2 is free
+      const uint32_t abase = tc::smem_u32(sm + S::OFF_A + s2 * S::A_STAGE);
       if (active) {
-        const double2* ey = reinterpret_cast<const double2*>(sm + S::OFF_F + s * S::F_STAGE) + KCP * D;
-        const double2* ez = ey + KCP * D;
-#pragma unroll 1
-        for (int kc = 0; kc < KB / 16; ++kc) {
+        const unsigned char* tb = sm + S::OFF_T + t * S::T_STRIDE;
+        const double2* ey = reinterpret_cast<const double2*>(tb + S::EY_OFF);
+        const double2* ez = reinterpret_cast<const double2*>(tb + S::EZ_OFF);
+        {
+          const int kc = kh;
           uint32_t w[4][4];
 #pragma unroll
           for (int p = 0; p < 4; ++p) {
             const int j0 = kc * 8 + 2 * p;
-            const double2 v0 = cmul_d(ez[j0 * (NK + 1) + kz], ey[j0 * D + ky]);
-            const double2 v1 = cmul_d(ez[(j0 + 1) * (NK + 1) + kz], ey[(j0 + 1) * D + ky]);
+            const double2 v0 = cmul_d(ez[j0 * S::EZS + kz], ey[j0 * D + ky]);
+            const double2 v1 = cmul_d(ez[(j0 + 1) * S::EZS + kz], ey[(j0 + 1) * D + ky]);
             uint32_t by[4];
             transpose4(fix24(v0.x), fix24(v0.y), fix24(v1.x), fix24(v1.y), by);
 #pragma unroll
@@ -362,31 +486,7 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
         }
       }
       tc::fence_async_smem();
-      if (c + 2 < nch) tc::bar_arrive(BAR_EMPTY0 + s, S::THREADS);
-      tc::bar_sync(BAR_CONS, RPC);
-      if (tid == 0 && !s_abort) {
-        tc::tc_fence_after();
-        const uint32_t bbase = tc::smem_u32(sm + S::OFF_B + s * S::B_STAGE);
-        constexpr uint32_t LBO_A = RPC * 16, LBO_B = NPAD * 16;
-#pragma unroll
-        for (int ks = 0; ks < S::KSTEPS; ++ks) {
-          const uint32_t ka = abase + ks * 2 * LBO_A;
-          const uint32_t kb = bbase + ks * 2 * LBO_B;
-          // slice products (a slice sa, b slice sb) of order sa + sb <= 3, into accumulator sa + sb
-#pragma unroll
-          for (int sa = 0; sa < 4; ++sa) {
-#pragma unroll
-            for (int sb2 = 0; sb2 + sa < 4; ++sb2) {
-              const int k = sa + sb2;
-              const uint32_t first = (c == 0 && ks == 0 && sa == 0) ? 0u : 1u;
-              tc::mma_i8(tmem + uint32_t(k * NPAD), tc::smem_desc(ka + sa * S::A_SLICE, LBO_A, 128),
-                         tc::smem_desc(kb + sb2 * S::B_SLICE, LBO_B, 128), tc::idesc_i8(RPC, NPAD), first);
-            }
-          }
-        }
-        tc::mma_commit(&mma_bar[s]);
-        last_commit = c;
-      }
+      tc::bar_arrive(BAR_AREADY0 + s2, S::THREADS);
     }
     // ------------------------------------------------------------ epilogue
     if (nch > 0) {
@@ -394,13 +494,13 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
       wait_bar(&mma_bar[cl & 1], uint32_t(cl >> 1) & 1);
     }
     tc::tc_fence_after();
-    tc::bar_sync(BAR_CONS, RPC);  // every consumer is past its last shared-memory read of the pipeline
-    const int q = warp & 3;       // TMEM lane quarter
+    tc::bar_sync(BAR_CONS, S::CTHREADS);  // every consumer is past its last read of the pipeline buffers
+    const int q = warp & 3;            // TMEM lane quarter (warps 4k .. 4k + 3 read lanes 0 .. 127)
     double2* stage = reinterpret_cast<double2*>(sm) + size_t(lr) * D;
     const double scale = qmax / (SL_SCALE * SL_SCALE);
     if (nch > 0 && !s_abort) {
 #pragma unroll 1
-      for (int cb = 0; cb < NPAD / 16; ++cb) {
+      for (int cb = kh; cb < NPAD / 16; cb += S::CPR) {
         uint32_t a0[16], a1[16], a2[16], a3[16];
         const uint32_t ta = tmem + (uint32_t(32 * q) << 16) + uint32_t(cb * 16);
         tc::tmem_ld16(ta, a0);
@@ -418,10 +518,10 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
         }
       }
     } else {
-      for (int n = 0; n < D; ++n) stage[n] = make_double2(0.0, 0.0);
+      for (int n = kh; n < D; n += S::CPR) stage[n] = make_double2(0.0, 0.0);
     }
     tc::fence_async_smem();
-    tc::bar_sync(BAR_CONS, RPC);
+    tc::bar_sync(BAR_CONS, S::CTHREADS);
     if (tid == 0) {
       tc::bulk_store(it.out + size_t(row0) * D, sm, uint32_t(nrows) * D * 16u);
       tc::bulk_commit();
@@ -430,8 +530,10 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
   }
   // copies and MMAs this CTA started have ended (bounded waits; they only
   // matter when a pipeline wait gave up) before its TMEM is released
-  if (ptid == 0 && last_tma >= 0) tc::mbar_wait(&tma_bar[last_tma & 1], uint32_t(last_tma >> 1) & 1);
-  if (tid == 0 && last_commit >= 0) tc::mbar_wait(&mma_bar[last_commit & 1], uint32_t(last_commit >> 1) & 1);
+  if (control && (tid & 31) == 0) {
+    if (last_fetch >= 0) tc::mbar_wait(&tma_bar[last_fetch % TSTAGES], uint32_t(last_fetch / TSTAGES) & 1);
+    if (last_commit >= 0) tc::mbar_wait(&mma_bar[last_commit & 1], uint32_t(last_commit >> 1) & 1);
+  }
   tc::tc_fence_before();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tmem, S::TCOLS);
@@ -457,12 +559,17 @@ __global__ void k_absmax(const double* __restrict__ q, int n, double* out) {
 }
 
 template <int NK>
-void launch_mixed(const CUtensorMap& tmap, const MixItem* d_items, int nitems, const double* d_qmax, int* d_err,
-                  cudaStream_t st) {
+void launch_mixed(const CUtensorMap& tmap, const MixItem* d_items, int nitems, const int2* d_chunks, int nchunks,
+                  const double* d_qmax, int* d_err, cudaStream_t st) {
   using S = MixShape<NK>;
   if (nitems == 0) return;
+  if (nchunks > 0) {
+    raise_smem_limit(reinterpret_cast<const void*>(k_pw_tables<NK>), S::TK_SMEM);
+    k_pw_tables<NK><<<unsigned(nchunks), S::TTHREADS, S::TK_SMEM, st>>>(tmap, d_items, d_chunks, d_qmax, d_err);
+    PDMK_LAUNCH_CHECK();
+  }
   raise_smem_limit(reinterpret_cast<const void*>(k_pw_mixed<NK>), S::SMEM);
-  k_pw_mixed<NK><<<unsigned(nitems), S::THREADS, S::SMEM, st>>>(tmap, d_items, d_qmax, d_err);
+  k_pw_mixed<NK><<<unsigned(nitems), S::THREADS, S::SMEM, st>>>(d_items, d_qmax, d_err);
   PDMK_LAUNCH_CHECK();
 }
 
@@ -489,6 +596,20 @@ int mixed_chunk(int nk) {
     case 17: return MixShape<17>::KCP;
     case 19: return MixShape<19>::KCP;
     case 26: return MixShape<26>::KCP;
+    default: throw std::invalid_argument("mixed precision: unsupported mode count");
+  }
+}
+
+int mixed_table_bytes(int nk) {
+  switch (nk) {
+    case 4: return MixShape<4>::T_BYTES;
+    case 6: return MixShape<6>::T_BYTES;
+    case 8: return MixShape<8>::T_BYTES;
+    case 12: return MixShape<12>::T_BYTES;
+    case 13: return MixShape<13>::T_BYTES;
+    case 17: return MixShape<17>::T_BYTES;
+    case 19: return MixShape<19>::T_BYTES;
+    case 26: return MixShape<26>::T_BYTES;
     default: throw std::invalid_argument("mixed precision: unsupported mode count");
   }
 }
@@ -527,19 +648,22 @@ void launch_absmax(const double* sq, int n, double* out, cudaStream_t st) {
   PDMK_LAUNCH_CHECK();
 }
 
-void dispatch_mixed(int nk, const CUtensorMap& tmap, const MixItem* d_items, int nitems, const double* d_qmax,
-                    int* d_err, cudaStream_t st) {
+void dispatch_mixed(int nk, const CUtensorMap& tmap, const MixItem* d_items, int nitems, const int2* d_chunks,
+                    int nchunks, const double* d_qmax, int* d_err, cudaStream_t st) {
+#define PDMK_MIX_CASE(n) \
+  case n: launch_mixed<n>(tmap, d_items, nitems, d_chunks, nchunks, d_qmax, d_err, st); break;
   switch (nk) {
-    case 4: launch_mixed<4>(tmap, d_items, nitems, d_qmax, d_err, st); break;
-    case 6: launch_mixed<6>(tmap, d_items, nitems, d_qmax, d_err, st); break;
-    case 8: launch_mixed<8>(tmap, d_items, nitems, d_qmax, d_err, st); break;
-    case 12: launch_mixed<12>(tmap, d_items, nitems, d_qmax, d_err, st); break;
-    case 13: launch_mixed<13>(tmap, d_items, nitems, d_qmax, d_err, st); break;
-    case 17: launch_mixed<17>(tmap, d_items, nitems, d_qmax, d_err, st); break;
-    case 19: launch_mixed<19>(tmap, d_items, nitems, d_qmax, d_err, st); break;
-    case 26: launch_mixed<26>(tmap, d_items, nitems, d_qmax, d_err, st); break;
+    PDMK_MIX_CASE(4)
+    PDMK_MIX_CASE(6)
+    PDMK_MIX_CASE(8)
+    PDMK_MIX_CASE(12)
+    PDMK_MIX_CASE(13)
+    PDMK_MIX_CASE(17)
+    PDMK_MIX_CASE(19)
+    PDMK_MIX_CASE(26)
     default: throw std::invalid_argument("mixed precision: unsupported mode count");
   }
+#undef PDMK_MIX_CASE
 }
 
 }  // namespace pdmk

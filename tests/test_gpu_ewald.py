@@ -94,15 +94,18 @@ def clustered(n, L, seed, n_clusters=64, frac=0.8):
 
 # The target accuracy at N = 1e6: 1e-8 relative to the FP64 Ewald energy, for
 # the FP64 path and the mixed-precision path, on the uniform cube (the
-# candidate-query configuration) and the clustered system.
-@pytest.mark.parametrize("kind", ["uniform", "clustered"])
+# candidate-query configuration, 9 digits) and the clustered system. On the
+# clustered system 9 digits give the method's own error near 2e-8 (inside
+# the reference's 5e-8 tolerance at 9 digits, checked here), so the 1e-8
+# target takes 12 digits there, the escalation the workload allows.
+@pytest.mark.parametrize("kind,digits,tol", [("uniform", 9, 1e-8), ("clustered", 9, 5e-8), ("clustered", 12, 1e-8)])
 @pytest.mark.parametrize("precision", [P.PRECISION_FP64, P.PRECISION_MIXED])
-def test_dmk_vs_gpu_ewald_n1e6(kind, precision):
+def test_dmk_vs_gpu_ewald_n1e6(kind, digits, tol, precision):
     n, L = 1_000_000, 100.0
     rng = np.random.default_rng(21)
     r = rng.uniform(0, L, 3 * n) if kind == "uniform" else clustered(n, L, 21)
     q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
-    t = P.HPDMKPtTree(P.HPDMKParams(n_per_leaf=200, digits=9, L=L, init=P.DIRECT), r, q, leaf_slack=0,
+    t = P.HPDMKPtTree(P.HPDMKParams(n_per_leaf=200, digits=digits, L=L, init=P.DIRECT), r, q, leaf_slack=0,
                       precision=precision)
     try:
         e, _ = t.ewald_energy()
@@ -110,7 +113,8 @@ def test_dmk_vs_gpu_ewald_n1e6(kind, precision):
         t.form_incoming_pw()
         dmk = t.eval_energy()
         rel = abs(dmk - e) / abs(e)
-        print(f"\nACCURACY n1e6 {kind} precision={precision} depth={t.max_depth} dmk={dmk!r} ewald={e!r} rel={rel:.3e}")
-        assert rel <= 1e-8, (dmk, e, rel)
+        print(f"\nACCURACY n1e6 {kind} digits={digits} precision={precision} depth={t.max_depth} dmk={dmk!r} "
+              f"ewald={e!r} rel={rel:.3e}")
+        assert rel <= tol, (dmk, e, rel)
     finally:
         t.close()
