@@ -340,93 +340,119 @@ __global__ void k_reduce_chunks(const double2* part, const int* chunk_first, con
 }
 
 // ---------------------------------------------------------------------------
-// inc_B = conj(out_B) + sum_C conj(out_C * exp(-i k.p L)) (form_incoming_pw,
-// src/planewave.cpp:99-155) for the 8 children of one parent at once: the
-// children's 27-box neighbourhoods lie in the 4x4x4 cube of boxes around the
-// parent, so a block stages the cube's outgoing rows for one tile of INC_KT
-// modes in shared memory (image phase applied, conjugated) and every child
-// sums its 27 cells from there. Each row tile crosses L2 once per cube
-// instead of once per receiving box. The energy partial of a block sums its
-// non-leaf children, which share one level.
-constexpr int INC_KT = 32;
+// inc_B = conj(out_B) + sum_C conj(out_C * exp(-i k.p L)) over B's 26
+// colleagues C (form_incoming_pw, src/planewave.cpp:99-155), for the
+// 4 x 4 x 4 boxes of level l below one box G of level l - 2 at once: their
+// 27-box neighbourhoods lie in the 6 x 6 x 6 cube of level-l cells around
+// them. A block stages the cube's outgoing rows for one tile of INC_KT modes
+// in shared memory (image phase applied; absent and empty cells are zero),
+// then each thread sums the 3 x 3 (y, z) neighbourhood of six x columns once
+// and slides the 3-wide x window over them for its 4 receivers. A row tile
+// crosses L2 216 / 64 = 3.4 times per receiving box (8 times with the
+// 4 x 4 x 4 cube around one parent). The energy partial of a block sums its
+// non-leaf receivers, which share one level.
+constexpr int INC_KT = 16;    // modes per tile
+constexpr int INC_T = 256;    // threads: INC_KT modes x 16 (y, z) lines of 4 receivers along x
+constexpr int INC_CELLS = 216;
+constexpr size_t INC_SMEM = sizeof(double2) * INC_CELLS * INC_KT + sizeof(int) * (INC_CELLS + 64) + INC_CELLS;
 
-// Grid: ngroups x slots blocks; block (slot, g) handles the tiles slot,
-// slot + slots, ... of group g, so its set-up (the cube's box list) is paid
-// once, and the groups sharing a slot walk the same tiles together (their
-// shared rows meet in L2).
-__global__ void __launch_bounds__(8 * INC_KT) k_incoming_sib(DevTree T, const int* __restrict__ parents, int ngroups,
-                                                              int slots, double* part) {
-  __shared__ double2 w[64][INC_KT];
-  __shared__ int s_src[64];
-  __shared__ signed char s_f[64][3];
+// rank of a refined cell within its level (Morton order)
+__device__ inline int refined_rank(const DevTree& T, int level, uint64_t cell) {
+  const uint32_t w = T.bm_d[level][cell >> 5];
+  return T.wprefix_d[level][cell >> 5] + __popc(w & ((1u << (cell & 31)) - 1u));
+}
+
+// Grid: ncubes x slots blocks; block (slot, c) handles the tiles slot,
+// slot + slots, ... of cube c, so its set-up (the cube's cell lookup) is
+// paid once, and the cubes sharing a slot walk the same tiles together (the
+// cells two neighbouring cubes share meet in L2).
+__global__ void __launch_bounds__(INC_T, 3) k_incoming_cube(DevTree T, const int* __restrict__ cubes, int ncubes,
+                                                          int slots, double* part) {
+  extern __shared__ double2 w[];                             // [INC_CELLS][INC_KT]
+  int* s_row = reinterpret_cast<int*>(w + INC_CELLS * INC_KT);  // outgoing row of each cell, -1: absent or empty
+  int* s_recv = s_row + INC_CELLS;                           // expansion row of each receiver, -1: none
+  unsigned char* s_wrap = reinterpret_cast<unsigned char*>(s_recv + 64);  // image flags, 2 bits per axis
   __shared__ double sm[32];
-  const int slot = blockIdx.x / ngroups, g = blockIdx.x % ngroups;
-  const int parent = parents[g];
-  const int c0 = T.node_child0[parent];
-  const int l = T.node_level[parent] + 1;
+  const int slot = blockIdx.x / ncubes, cb = blockIdx.x % ncubes;
+  const int G = cubes[cb];
+  const int l = T.node_level[G] + 2;
+  const int side = 1 << l;
+  const uint64_t gp = T.node_prefix[G];
+  const int O[3] = {4 * int(compact3(gp)), 4 * int(compact3(gp >> 1)), 4 * int(compact3(gp >> 2))};
   const int base = T.pw_base;
-  const uint64_t pp = T.node_prefix[parent];
-  const int P[3] = {int(compact3(pp)), int(compact3(pp >> 1)), int(compact3(pp >> 2))};
-  if (threadIdx.x < 64) {
-    const int t = int(threadIdx.x);
-    s_src[t] = -1;
-    const int o[3] = {t & 3, (t >> 2) & 3, t >> 4};
+  if (threadIdx.x < INC_CELLS) {
+    const int t = threadIdx.x;
+    const int c[3] = {t % 6 - 1, (t / 6) % 6 - 1, t / 36 - 1};
+    int g[3];
+    unsigned wrap = 0;
     for (int a = 0; a < 3; ++a) {
-      const int v = 2 * P[a] - 1 + o[a];
-      s_f[t][a] = static_cast<signed char>(v < 0 ? -1 : (v >= (1 << l) ? 1 : 0));
+      int v = O[a] + c[a];
+      const int f = v < 0 ? 1 : (v >= side ? 2 : 0);  // 1: image below (-1), 2: above (+1)
+      v = f == 1 ? v + side : (f == 2 ? v - side : v);
+      g[a] = v;
+      wrap |= unsigned(f) << (2 * a);
     }
+    const uint64_t m = morton3(uint32_t(g[0]), uint32_t(g[1]), uint32_t(g[2]));
+    int node = -1;
+    if ((T.bm_d[l - 1][m >> 8] >> ((m >> 3) & 31)) & 1u)
+      node = T.level_start_d[l] + 8 * refined_rank(T, l - 1, m >> 3) + int(m & 7);
+    s_row[t] = (node >= 0 && T.node_count[node] > 0) ? node - base : -1;
+    s_wrap[t] = static_cast<unsigned char>(wrap);
+    if (c[0] >= 0 && c[0] < 4 && c[1] >= 0 && c[1] < 4 && c[2] >= 0 && c[2] < 4)
+      s_recv[c[0] + 4 * c[1] + 16 * c[2]] = (node >= 0 && T.node_child0[node] >= 0) ? node - base : -1;
   }
   __syncthreads();
-  // cube cells from the children's colleague lists (a cell seen from two
-  // children names the same box)
-  if (threadIdx.x < 216) {
-    const int c = threadIdx.x / 27, dir = threadIdx.x % 27;
-    const int child = c0 + c;
-    const int j = dir == 13 ? child : T.col27[size_t(child) * 27 + dir];
-    const int cell = ((c & 1) + 1 + dir % 3 - 1) + 4 * (((c >> 1) & 1) + 1 + (dir / 3) % 3 - 1) +
-                     16 * (((c >> 2) & 1) + 1 + dir / 9 - 1);
-    if (j >= 0 && T.node_count[j] > 0) s_src[cell] = j - base;
-  }
   const int n = T.n_diff, d = T.dd;
   const int two_l = (l & 1) ? 2 : 1;
-  const int kk = threadIdx.x % INC_KT, part8 = threadIdx.x / INC_KT;  // staging: one mode, cells part8 + 8 i
-  const int c = part8;                                                // summing: child c
-  const int child = c0 + c;
-  const bool recv = T.node_child0[child] >= 0;
-  const int cx = (c & 1) + 1, cy = ((c >> 1) & 1) + 1, cz = ((c >> 2) & 1) + 1;
-  __syncthreads();
+  const int kk = threadIdx.x % INC_KT;
+  const int line = threadIdx.x / INC_KT, ry = line & 3, rz = line >> 2;
   double e = 0;
   const int ktiles = (T.H + INC_KT - 1) / INC_KT;
   for (int tile = slot; tile < ktiles; tile += slots) {
     const int k = tile * INC_KT + kk;
     const bool kin = k < T.H;
     const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
-    const int a0 = ((ix - n) % 3 + 3) % 3, a1 = ((iy - n) % 3 + 3) % 3, a2 = ((iz - n) % 3 + 3) % 3;
-    double2 v[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int row = s_src[part8 + 8 * i];
-      v[i] = (row >= 0 && kin) ? T.out[size_t(row) * T.H + k] : make_double2(0.0, 0.0);
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int cell = part8 + 8 * i;
-      const signed char* f = s_f[cell];
-      // exp(-i 2 pi sgn / 3) = w6^{-2 sgn}, sgn = (k - n).f 2^l; the sum lies in [-12, 12]
-      const int e3 = ((a0 * f[0] + a1 * f[1] + a2 * f[2]) * two_l + 12) % 3;
-      w[cell][kk] = cconj(e3 == 0 ? v[i] : cmul(v[i], root6(-2 * e3)));
+    const int a[3] = {((ix - n) % 3 + 3) % 3, ((iy - n) % 3 + 3) % 3, ((iz - n) % 3 + 3) % 3};
+    // stage the cube: mode kk of cells line, line + 16, ...
+    for (int c = line; c < INC_CELLS; c += INC_T / INC_KT) {
+      const int row = s_row[c];
+      double2 v = (row >= 0 && kin) ? T.out[size_t(row) * T.H + k] : make_double2(0.0, 0.0);
+      const unsigned wr = s_wrap[c];
+      if (wr) {
+        // image phase exp(-i 2 pi sgn / 3) = w6^{-2 sgn}, sgn = (k - n).f 2^l;
+        // the sum lies in [-12, 12]
+        int sg = 0;
+        for (int ax = 0; ax < 3; ++ax) {
+          const unsigned f = (wr >> (2 * ax)) & 3u;
+          sg += f == 1 ? -a[ax] : (f == 2 ? a[ax] : 0);
+        }
+        const int e3 = (sg * two_l + 12) % 3;
+        if (e3) v = cmul(v, root6(-2 * e3));
+      }
+      w[c * INC_KT + kk] = v;
     }
     __syncthreads();
-    if (kin && recv) {
+    // the 3 x 3 (y, z) sums of the six x columns of this thread's line
+    double2 col[6];
+#pragma unroll
+    for (int cx = 0; cx < 6; ++cx) {
       double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-      for (int dir = 0; dir < 27; ++dir) {
-        const int cell = (cx + dir % 3 - 1) + 4 * (cy + (dir / 3) % 3 - 1) + 16 * (cz + dir / 9 - 1);
-        acc = cadd(acc, w[cell][kk]);
+      for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy) acc = cadd(acc, w[((rz + dz) * 36 + (ry + dy) * 6 + cx) * INC_KT + kk]);
+      col[cx] = acc;
+    }
+    if (kin) {
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        const int rrow = s_recv[x + 4 * ry + 16 * rz];
+        if (rrow < 0) continue;
+        const double2 inc = cconj(cadd(cadd(col[x], col[x + 1]), col[x + 2]));
+        T.inc[size_t(rrow) * T.H + k] = inc;
+        const double2 o = w[((rz + 1) * 36 + (ry + 1) * 6 + x + 1) * INC_KT + kk];  // the receiver's own row
+        e += (o.x * inc.x - o.y * inc.y) * T.D2[k];
       }
-      T.inc[size_t(child - base) * T.H + k] = acc;
-      const double2 o = T.out[size_t(child - base) * T.H + k];
-      e += (o.x * acc.x - o.y * acc.y) * T.D2[k];
     }
     __syncthreads();
   }
@@ -434,17 +460,17 @@ __global__ void __launch_bounds__(8 * INC_KT) k_incoming_sib(DevTree T, const in
   if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
-// E_diff from the sibling-tiled partials: sum over groups C_l dscale_l
-// sum_tiles part, minus sum over non-leaf boxes Q_B S_l
-__global__ void k_diff_finish_sib(DevTree T, const int* __restrict__ parents, int ngroups, int ktiles,
-                                  const double* part, const int* __restrict__ boxes, int nboxes, const double* q2,
-                                  const double* Cl, const double* Sl, double* out) {
+// E_diff from the cube-tiled partials: sum over cubes C_l dscale_l
+// sum_slots part, minus sum over non-leaf boxes Q_B S_l
+__global__ void k_diff_finish_cube(DevTree T, const int* __restrict__ cubes, int ncubes, int slots,
+                                   const double* part, const int* __restrict__ boxes, int nboxes, const double* q2,
+                                   const double* Cl, const double* Sl, double* out) {
   __shared__ double sm[32];
   double e = 0;
-  for (int g = threadIdx.x; g < ngroups; g += blockDim.x) {
-    const int l = T.node_level[parents[g]] + 1;
+  for (int c = threadIdx.x; c < ncubes; c += blockDim.x) {
+    const int l = T.node_level[cubes[c]] + 2;
     double t = 0;
-    for (int tile = 0; tile < ktiles; ++tile) t += part[size_t(tile) * ngroups + g];
+    for (int sl = 0; sl < slots; ++sl) t += part[size_t(sl) * ncubes + c];
     e += Cl[l] * level_dscale(l) * t;
   }
   for (int b = threadIdx.x; b < nboxes; b += blockDim.x) e -= q2[b] * Sl[T.node_level[boxes[b]]];
@@ -862,7 +888,7 @@ size_t DmkTree::partials_needed() const {
   long n_pw = D.pw_hi >= D.pw_lo ? long(D.level_start[D.pw_hi + 1]) - D.level_start[D.pw_lo] : 0;
   long ktiles = (D.H + TPB - 1) / TPB;
   need = std::max<size_t>(need, size_t(n_pw) * ktiles + 2 * size_t(n_pw) + 64);
-  // sibling-tiled incoming: at most one group per 8 expansion boxes
+  // cube-tiled incoming: at most one cube per 8 expansion boxes
   need = std::max<size_t>(need, size_t((D.H + INC_KT - 1) / INC_KT) * size_t(n_pw / 8 + 1) + 2 * size_t(n_pw) + 64);
   need = std::max<size_t>(need, size_t(D.n_nodes) * RES_NY_MAX + 64);
   return need;
@@ -1156,18 +1182,23 @@ void DmkTree::build_box_lists(const std::vector<int>& c0) {
   std::vector<int> leaves;
   for (int id = D.level_start[2]; id < D.n_nodes; ++id)
     if (c0[id] < 0) leaves.push_back(id);
-  // parents whose children carry expansions and include a non-leaf box
-  std::vector<int> groups;
+  // boxes two levels above the expansion levels with a non-leaf grandchild:
+  // each names the 4 x 4 x 4 receiving boxes of one incoming block
+  std::vector<int> cubes;
   if (D.pw_hi >= D.pw_lo)
-    for (int id = D.level_start[D.pw_lo - 1]; id < D.level_start[D.pw_hi]; ++id) {
+    for (int id = D.level_start[D.pw_lo - 2]; id < D.level_start[D.pw_hi - 1]; ++id) {
       if (c0[id] < 0) continue;
       bool any = false;
-      for (int c = 0; c < 8; ++c) any = any || c0[c0[id] + c] >= 0;
-      if (any) groups.push_back(id);
+      for (int a = 0; a < 8 && !any; ++a) {
+        const int ch = c0[id] + a;
+        if (c0[ch] < 0) continue;
+        for (int b = 0; b < 8; ++b) any = any || c0[c0[ch] + b] >= 0;
+      }
+      if (any) cubes.push_back(id);
     }
-  n_groups_ = int(groups.size());
-  d_groups_ = static_cast<int*>(alloc(sizeof(int) * (n_groups_ + 1)));
-  PDMK_CUDA(cudaMemcpyAsync(d_groups_, groups.data(), sizeof(int) * n_groups_, cudaMemcpyHostToDevice, st_));
+  n_cubes_ = int(cubes.size());
+  d_cubes_ = static_cast<int*>(alloc(sizeof(int) * (n_cubes_ + 1)));
+  PDMK_CUDA(cudaMemcpyAsync(d_cubes_, cubes.data(), sizeof(int) * n_cubes_, cudaMemcpyHostToDevice, st_));
   n_nonleaf_ = int(nonleaf.size());
   n_leaves_ = int(leaves.size());
   d_nonleaf_ = static_cast<int*>(alloc(sizeof(int) * (n_nonleaf_ + 1)));
@@ -1203,19 +1234,24 @@ void DmkTree::run_incoming(bool write_inc) {
     return;
   }
   const int ktiles = (D.H + TPB - 1) / TPB;
-  const size_t n_part = std::max(size_t(ktiles) * n_nonleaf_, size_t((D.H + INC_KT - 1) / INC_KT) * n_groups_);
+  const size_t n_part = std::max(size_t(ktiles) * n_nonleaf_, size_t((D.H + INC_KT - 1) / INC_KT) * n_cubes_);
   double* part = D.partials;
   double* q2 = D.partials + n_part;
   k_box_q2<<<unsigned(n_nonleaf_), TPB, 0, st_>>>(D, d_nonleaf_, q2);
   PDMK_LAUNCH_CHECK();
   if (write_inc) {
-    // about four resident waves of blocks, each walking a strided set of tiles
+    // about inc_waves resident waves of blocks (three per SM), each walking a
+    // strided set of tiles
     const int kt = (D.H + INC_KT - 1) / INC_KT;
-    const int slots = std::max(1, std::min(kt, (tune_.inc_waves * 8 * 148 + n_groups_ - 1) / n_groups_));
-    k_incoming_sib<<<unsigned(slots * n_groups_), 8 * INC_KT, 0, st_>>>(D, d_groups_, n_groups_, slots, part);
-    PDMK_LAUNCH_CHECK();
-    k_diff_finish_sib<<<1, 1024, 0, st_>>>(D, d_groups_, n_groups_, slots, part, d_nonleaf_, n_nonleaf_, q2, d_Cl_,
-                                           d_Sl_, d_scalars_ + 1);
+    const int nc = std::max(n_cubes_, 1);
+    const int slots = std::max(1, std::min(kt, (tune_.inc_waves * 3 * 148 + nc - 1) / nc));
+    if (n_cubes_ > 0) {
+      raise_smem_limit(reinterpret_cast<const void*>(k_incoming_cube), INC_SMEM);
+      k_incoming_cube<<<unsigned(slots * n_cubes_), INC_T, INC_SMEM, st_>>>(D, d_cubes_, n_cubes_, slots, part);
+      PDMK_LAUNCH_CHECK();
+    }
+    k_diff_finish_cube<<<1, 1024, 0, st_>>>(D, d_cubes_, n_cubes_, slots, part, d_nonleaf_, n_nonleaf_, q2, d_Cl_,
+                                            d_Sl_, d_scalars_ + 1);
     PDMK_LAUNCH_CHECK();
   } else {
     k_tridot<<<unsigned(ktiles * n_nonleaf_), TPB, 0, st_>>>(D, d_nonleaf_, n_nonleaf_, part);

@@ -43,10 +43,13 @@
 //     box reads these once-formed tables.
 //   - k_pw_mixed, one CTA per 128-row M tile of a box (or split-K chunk): a
 //     control warp brings each chunk's table block into shared memory with a
-//     bulk copy (three chunks in flight) and issues the MMAs; the consumer
-//     warps form A = ez ey in FP64, one thread per output row (kz, ky) and
-//     group of 8 particles, and slice it; the A stages are double-buffered, so the tensor
-//     core works on chunk c while the consumers build chunk c + 1; the
+//     bulk copy (three or four chunks in flight) and issues the MMAs, A from
+//     tensor memory and B from shared memory; the consumer warps form
+//     A = ez ey in FP64, one thread per output row (kz, ky) and group of 8
+//     particles, slice it and store the slices into tensor memory
+//     (tcgen05.st), which keeps A's traffic off shared memory; the A stages
+//     are double-buffered, so the tensor core works on chunk c while the
+//     consumers build chunk c + 1; the
 //     epilogue reads the accumulators (tcgen05.ld), combines them in FP64,
 //     stages the rows in shared memory and writes them with one bulk copy
 //     into the box's expansion row range, which is contiguous in HBM.
@@ -69,7 +72,7 @@ namespace {
 
 constexpr int RPC = 128;           // rows (one M tile) per CTA
 constexpr int NACC = 4;            // accumulators: slice-product orders s + t = 2 .. 5
-constexpr int TSTAGES = 3;         // table blocks in flight per CTA
+constexpr int SMEM_MAX = 227 * 1024;
 
 __host__ __device__ constexpr int npad_of(int nk) { return (2 * (2 * nk + 1) + 15) / 16 * 16; }
 __host__ __device__ constexpr int ezs_of(int nk) { return (nk + 1) | 1; }
@@ -77,21 +80,24 @@ __host__ __device__ constexpr int ezs_of(int nk) { return (nk + 1) | 1; }
 __host__ __device__ constexpr int table_bytes(int nk, int kcp) {
   return 4 * npad_of(nk) * 2 * kcp + kcp * ((2 * nk + 1) + ezs_of(nk)) * 16;
 }
-// shared memory of the contraction kernel for chunks of kcp particles
-__host__ __device__ constexpr int mix_smem_bytes(int nk, int kcp) {
-  return 2 * 4 * RPC * 2 * kcp + TSTAGES * ((table_bytes(nk, kcp) + 127) / 128 * 128) + 1024;
+__host__ __device__ constexpr int table_stride(int nk, int kcp) { return (table_bytes(nk, kcp) + 127) / 128 * 128; }
+// TMEM columns: the four accumulators, then two A stages of 2 kcp columns
+// (four slices of 2 kcp bytes per row, four bytes to a column)
+__host__ __device__ constexpr int tmem_cols(int nk, int kcp) { return NACC * npad_of(nk) + 2 * 2 * kcp; }
+// chunks of 32 particles when three table stages and the TMEM columns fit
+__host__ __device__ constexpr bool chunk32_fits(int nk) {
+  return 3 * table_stride(nk, 32) + 1024 <= SMEM_MAX && tmem_cols(nk, 32) <= 512;
 }
 
 template <int NK>
 struct MixShape {
   static constexpr int D = 2 * NK + 1;
-  static constexpr int ROWS = (NK + 1) * D;
+  static constexpr int ROWS = (NK + 1) * D;  // row r = kz D + ky, as the expansion's layout
   static constexpr int NPAD = npad_of(NK);  // MMA N: Re columns [0, D), Im columns [HALF, HALF + D)
   static constexpr int HALF = NPAD / 2;
   static constexpr int EZS = ezs_of(NK);    // odd row strides keep 16-byte stores on distinct bank groups
   static constexpr int TILES = (ROWS + RPC - 1) / RPC;  // CTAs per box
-  // particles per chunk: 32 when the stages fit, else 16
-  static constexpr int KCP = mix_smem_bytes(NK, 32) <= 227 * 1024 ? 32 : 16;
+  static constexpr int KCP = chunk32_fits(NK) ? 32 : 16;  // particles per chunk
   static constexpr int KB = 2 * KCP;        // K bytes per chunk (real and imaginary part per particle)
   static constexpr int KSTEPS = KB / 32;    // MMA K steps (32 bytes each) per chunk
   static constexpr int CPR = KB / 16;            // consumer threads per row: one per 16-byte K group (8 particles)
@@ -100,31 +106,35 @@ struct MixShape {
   static constexpr int TTHREADS = 6 * KCP;       // table kernel: one thread per (particle, axis, half)
   static constexpr int COORD_BOX = KCP + 2;      // TMA box along the slots: even start, one spare each side
   static constexpr int COORD_BYTES = 4 * COORD_BOX * 8;
-  static constexpr int TCOLS_USED = NACC * NPAD;
+  // TMEM: accumulators at columns [0, NACC NPAD), A stage s slice t at
+  // columns A_COL0 + s KB + t KB / 4 (lane = row)
+  static constexpr int A_COL0 = NACC * NPAD;
+  static constexpr int TCOLS_USED = tmem_cols(NK, KCP);
   static constexpr int TCOLS = TCOLS_USED <= 32 ? 32 : TCOLS_USED <= 64 ? 64 : TCOLS_USED <= 128 ? 128
                                : TCOLS_USED <= 256 ? 256 : 512;
   // one chunk's table block
-  static constexpr int B_SLICE = NPAD * KB;
-  static constexpr int B_BYTES = 4 * B_SLICE;
+  // B: the four slices side by side along N ([16-byte K group][slice][column]
+  // [16 bytes]), so that one MMA can take up to BGROUP consecutive slices
+  static constexpr int B_KGROUP = 4 * NPAD * 16;  // bytes per 16-byte K group
+  static constexpr int B_BYTES = (KB / 16) * B_KGROUP;
+  static constexpr int BGROUP = 3 * NPAD <= 256 ? 3 : 2;  // slices per MMA (N <= 256)
+  // then the FP64 factors (double2): ey [particle][ky], ez [particle][kz]
   static constexpr int EY_OFF = B_BYTES;
   static constexpr int EZ_OFF = EY_OFF + KCP * D * 16;
   static constexpr int T_BYTES = EZ_OFF + KCP * EZS * 16;
-  static constexpr int T_STRIDE = (T_BYTES + 127) / 128 * 128;
-  // contraction kernel shared memory
-  static constexpr int A_SLICE = RPC * KB;
-  static constexpr int A_STAGE = 4 * A_SLICE;
-  static constexpr int OFF_A = 0;
-  static constexpr int OFF_T = OFF_A + 2 * A_STAGE;
-  static constexpr int PIPE_BYTES = OFF_T + TSTAGES * T_STRIDE;
-  static constexpr int STAGE_OUT = RPC * D * 16;  // epilogue staging, reuses the pipeline buffers
+  static constexpr int T_STRIDE = table_stride(NK, KCP);
+  // contraction kernel shared memory: the table stages (four when they fit)
+  static constexpr int TSTAGES = 4 * T_STRIDE + 1024 <= SMEM_MAX ? 4 : 3;
+  static constexpr int PIPE_BYTES = TSTAGES * T_STRIDE;
+  static constexpr int STAGE_OUT = RPC * D * 16;  // epilogue staging, reuses the table stages
   static constexpr int SMEM = (PIPE_BYTES > STAGE_OUT ? PIPE_BYTES : STAGE_OUT) + 1024;  // + alignment slack
   // table kernel shared memory: coordinates, ex scratch, the block
   static constexpr int TK_OFF_EX = (COORD_BYTES + 127) / 128 * 128;
   static constexpr int TK_OFF_T = (TK_OFF_EX + KCP * D * 16 + 127) / 128 * 128;
   static constexpr int TK_SMEM = TK_OFF_T + T_STRIDE + 1024;
-  static_assert(TCOLS_USED <= 512, "accumulators exceed TMEM");
+  static_assert(TCOLS_USED <= 512, "accumulators and A stages exceed TMEM");
   static_assert(HALF >= D, "imaginary columns overlap the real ones");
-  static_assert(SMEM <= 227 * 1024 && TK_SMEM <= 227 * 1024, "shared memory");
+  static_assert(SMEM <= SMEM_MAX && TK_SMEM <= SMEM_MAX, "shared memory");
   static_assert(KB % 32 == 0, "chunks are whole MMA K steps");
   static_assert(T_BYTES % 16 == 0, "bulk copies move multiples of 16 bytes");
 };
@@ -262,10 +272,9 @@ __device__ void axis_factors_d(double xr, double dk, int M, int X, int m0, int c
 
 
 // Table pass: the FP64 phase factors of one chunk of one box, the sliced B
-// operand in the tensor core's K-major layout ([slice][16-byte K group][column]
-// [16 bytes]) and the ey, ez factors ([particle][mode], double2), written to
-// the chunk's table block. One thread per (particle, axis, half of the mode
-// range), consecutive lanes on consecutive particles.
+// operand in the tensor core's K-major layout and the ey, ez factors,
+// written to the chunk's table block. One thread per (particle, axis, half
+// of the mode range), consecutive lanes on consecutive particles.
 template <int NK>
 __global__ void __launch_bounds__(MixShape<NK>::TTHREADS)
     k_pw_tables(const __grid_constant__ CUtensorMap coords, const MixItem* __restrict__ items,
@@ -317,9 +326,9 @@ __global__ void __launch_bounds__(MixShape<NK>::TTHREADS)
     }
   }
   __syncthreads();
-  // B operand from ex: column n < D is the real part of mode kx = n, column
-  // HALF + kx its imaginary part; K rows (2j, 2j+1) carry (Br, -Bi) for a
-  // real column and (Bi, Br) for an imaginary one
+  // B operand from ex: column n < D of each slice is the real part of mode
+  // kx = n, column HALF + kx its imaginary part; K rows (2j, 2j+1) carry
+  // (Br, -Bi) for a real column and (Bi, Br) for an imaginary one
   const uint32_t bbase = tc::smem_u32(blk);
   for (int task = tid; task < NPAD * (KB / 16); task += S::TTHREADS) {
     const int n = task % NPAD, kc = task / NPAD;
@@ -342,7 +351,7 @@ __global__ void __launch_bounds__(MixShape<NK>::TTHREADS)
     }
 #pragma unroll
     for (int sl = 0; sl < 4; ++sl)
-      st_shared_v4(bbase + sl * S::B_SLICE + kc * (NPAD * 16) + n * 16, w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
+      st_shared_v4(bbase + kc * S::B_KGROUP + (sl * NPAD + n) * 16, w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
   }
   tc::fence_async_smem();
   __syncthreads();
@@ -359,13 +368,13 @@ template <int NK>
 __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
     k_pw_mixed(const MixItem* __restrict__ items, const double* __restrict__ qmax_p, int* __restrict__ err) {
   using S = MixShape<NK>;
-  constexpr int D = S::D, NPAD = S::NPAD, HALF = S::HALF, KCP = S::KCP;
+  constexpr int D = S::D, NPAD = S::NPAD, HALF = S::HALF, KCP = S::KCP, KB = S::KB;
   extern __shared__ unsigned char smem_raw[];
   // the 1024-aligned base as an offset from the shared array, so that the
   // compiler keeps shared-memory (not generic) loads and stores
   unsigned char* sm = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
   __shared__ __align__(8) uint64_t mma_bar[2];
-  __shared__ __align__(8) uint64_t tma_bar[TSTAGES];
+  __shared__ __align__(8) uint64_t tma_bar[4];
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
 
@@ -381,7 +390,7 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
   if (tid == 0) {
     tc::mbar_init(&mma_bar[0], 1);
     tc::mbar_init(&mma_bar[1], 1);
-    for (int i = 0; i < TSTAGES; ++i) tc::mbar_init(&tma_bar[i], 1);
+    for (int i = 0; i < S::TSTAGES; ++i) tc::mbar_init(&tma_bar[i], 1);
     tc::mbar_fence_init();
     s_abort = 0;
   }
@@ -399,9 +408,9 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
     }
   };
   auto fetch = [&](int c) {  // chunk c's table block into table stage c % TSTAGES
-    const int t = c % TSTAGES;
+    const int t = c % S::TSTAGES;
     tc::mbar_arrive_expect_tx(&tma_bar[t], S::T_BYTES);
-    tc::bulk_load(sm + S::OFF_T + t * S::T_STRIDE, it.tab + size_t(c) * S::T_BYTES, S::T_BYTES, &tma_bar[t]);
+    tc::bulk_load(sm + t * S::T_STRIDE, it.tab + size_t(c) * S::T_BYTES, S::T_BYTES, &tma_bar[t]);
   };
   int last_fetch = -1;   // the last chunk requested (control lane 0)
   int last_commit = -1;  // the last chunk whose MMAs were committed (control lane 0)
@@ -410,30 +419,33 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
     // ------------------------------------------------------------ control warp
     const bool lead = (tid & 31) == 0;
     if (lead)
-      for (int c = 0; c < min(TSTAGES, nch); ++c) {
+      for (int c = 0; c < min(S::TSTAGES, nch); ++c) {
         fetch(c);
         last_fetch = c;
       }
     for (int c = 0; c < nch; ++c) {
-      const int s2 = c & 1, t = c % TSTAGES;
-      tc::bar_sync(BAR_AREADY0 + s2, S::THREADS);  // A of chunk c is in shared memory (and its tables landed)
+      const int s2 = c & 1, t = c % S::TSTAGES;
+      tc::bar_sync(BAR_AREADY0 + s2, S::THREADS);  // A of chunk c is in TMEM (and its tables landed)
       if (lead && !s_abort) {
         tc::tc_fence_after();
-        const uint32_t abase = tc::smem_u32(sm + S::OFF_A + s2 * S::A_STAGE);
-        const uint32_t bbase = tc::smem_u32(sm + S::OFF_T + t * S::T_STRIDE);
-        constexpr uint32_t LBO_A = RPC * 16, LBO_B = NPAD * 16;
+        const uint32_t abase = tmem + uint32_t(S::A_COL0 + s2 * KB);
+        // descriptor of the stage's B; the others differ by constant address offsets
+        const uint64_t bdesc = tc::smem_desc(tc::smem_u32(sm + t * S::T_STRIDE), S::B_KGROUP, 128);
+        const uint32_t acc0 = c > 0 ? 1u : 0u;
 #pragma unroll
         for (int ks = 0; ks < S::KSTEPS; ++ks) {
-          const uint32_t ka = abase + ks * 2 * LBO_A;
-          const uint32_t kb = bbase + ks * 2 * LBO_B;
-          // slice products (a slice sa, b slice sb) of order sa + sb <= 3, into accumulator sa + sb
+          // slice products (a slice sa, b slices sb) of order sa + sb <= 3 into
+          // accumulators sa + sb: one MMA per run of up to BGROUP b slices,
+          // whose accumulators are adjacent in TMEM as the slices are in B
 #pragma unroll
           for (int sa = 0; sa < 4; ++sa) {
 #pragma unroll
-            for (int sb = 0; sb + sa < 4; ++sb) {
-              const uint32_t first = (c == 0 && ks == 0 && sa == 0) ? 0u : 1u;
-              tc::mma_i8(tmem + uint32_t((sa + sb) * NPAD), tc::smem_desc(ka + sa * S::A_SLICE, LBO_A, 128),
-                         tc::smem_desc(kb + sb * S::B_SLICE, LBO_B, 128), tc::idesc_i8(RPC, NPAD), first);
+            for (int sb = 0; sb < 4 - sa; sb += S::BGROUP) {
+              const int nb = min(S::BGROUP, 4 - sa - sb);
+              const uint32_t acc = (ks == 0 && sa == 0) ? acc0 : 1u;
+              const uint64_t bd = bdesc + uint64_t((ks * 2 * S::B_KGROUP + sb * NPAD * 16) >> 4);
+              tc::mma_i8_ts(tmem + uint32_t((sa + sb) * NPAD), abase + uint32_t(sa * (KB / 4) + ks * 8), bd,
+                            tc::idesc_i8(RPC, nb * NPAD), acc);
             }
           }
         }
@@ -441,11 +453,11 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
         last_commit = c;
         // the table stage of chunk c is free once these MMAs have read its B
         // (the consumers are past its factors: they signalled above)
-        if (c + TSTAGES < nch) {
+        if (c + S::TSTAGES < nch) {
           wait_bar(&mma_bar[s2], uint32_t(c >> 1) & 1);
           if (!s_abort) {
-            fetch(c + TSTAGES);
-            last_fetch = c + TSTAGES;
+            fetch(c + S::TSTAGES);
+            last_fetch = c + S::TSTAGES;
           }
         }
       }
@@ -453,39 +465,42 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
     }
   } else {
     // ------------------------------------------------------------ consumers
-    const int lr = tid & (RPC - 1);  // local row
+    const int lr = tid & (RPC - 1);  // local row = TMEM lane
     const int kh = tid / RPC;        // this thread's 16-byte K group (8 particles) of each chunk
     const int r = row0 + lr;
     const bool active = lr < nrows;
     const int kz = active ? r / D : 0, ky = active ? r % D : 0;
+    // this thread's four A columns of slice 0 of stage 0 (its warp's lane quarter)
+    const uint32_t arow = tmem + (uint32_t(32 * (warp & 3)) << 16) + uint32_t(S::A_COL0 + kh * 4);
     for (int c = 0; c < nch; ++c) {
-      const int s2 = c & 1, t = c % TSTAGES;
-      wait_bar(&tma_bar[t], uint32_t(c / TSTAGES) & 1);    // this chunk's tables have landed
-      if (c >= 2) wait_bar(&mma_bar[s2], uint32_t((c >> 1) - 1) & 1);  // A stage s2 is free
-      const uint32_t abase = tc::smem_u32(sm + S::OFF_A + s2 * S::A_STAGE);
+      const int s2 = c & 1, t = c % S::TSTAGES;
+      wait_bar(&tma_bar[t], uint32_t(c / S::TSTAGES) & 1);    // this chunk's tables have landed
+      if (c >= 2) {
+        wait_bar(&mma_bar[s2], uint32_t((c >> 1) - 1) & 1);  // A stage s2 is free
+        tc::tc_fence_after();
+      }
+      uint32_t w[4][4] = {};
       if (active) {
-        const unsigned char* tb = sm + S::OFF_T + t * S::T_STRIDE;
+        const unsigned char* tb = sm + t * S::T_STRIDE;
         const double2* ey = reinterpret_cast<const double2*>(tb + S::EY_OFF);
         const double2* ez = reinterpret_cast<const double2*>(tb + S::EZ_OFF);
-        {
-          const int kc = kh;
-          uint32_t w[4][4];
 #pragma unroll
-          for (int p = 0; p < 4; ++p) {
-            const int j0 = kc * 8 + 2 * p;
-            const double2 v0 = cmul_d(ez[j0 * S::EZS + kz], ey[j0 * D + ky]);
-            const double2 v1 = cmul_d(ez[(j0 + 1) * S::EZS + kz], ey[(j0 + 1) * D + ky]);
-            uint32_t by[4];
-            transpose4(fix24(v0.x), fix24(v0.y), fix24(v1.x), fix24(v1.y), by);
+        for (int p = 0; p < 4; ++p) {
+          const int j0 = kh * 8 + 2 * p;
+          const double2 v0 = cmul_d(ez[j0 * S::EZS + kz], ey[j0 * D + ky]);
+          const double2 v1 = cmul_d(ez[(j0 + 1) * S::EZS + kz], ey[(j0 + 1) * D + ky]);
+          uint32_t by[4];
+          transpose4(fix24(v0.x), fix24(v0.y), fix24(v1.x), fix24(v1.y), by);
 #pragma unroll
-            for (int sl = 0; sl < 4; ++sl) w[sl][p] = by[3 - sl];
-          }
-#pragma unroll
-          for (int sl = 0; sl < 4; ++sl)
-            st_shared_v4(abase + sl * S::A_SLICE + kc * (RPC * 16) + lr * 16, w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
+          for (int sl = 0; sl < 4; ++sl) w[sl][p] = by[3 - sl];
         }
       }
-      tc::fence_async_smem();
+      // every lane stores (rows past the tile's end store zeros, never read back)
+#pragma unroll
+      for (int sl = 0; sl < 4; ++sl)
+        tc::tmem_st4(arow + uint32_t(s2 * KB + sl * (KB / 4)), w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
+      tc::tmem_st_wait();
+      tc::tc_fence_before();
       tc::bar_arrive(BAR_AREADY0 + s2, S::THREADS);
     }
     // ------------------------------------------------------------ epilogue
@@ -531,7 +546,7 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
   // copies and MMAs this CTA started have ended (bounded waits; they only
   // matter when a pipeline wait gave up) before its TMEM is released
   if (control && (tid & 31) == 0) {
-    if (last_fetch >= 0) tc::mbar_wait(&tma_bar[last_fetch % TSTAGES], uint32_t(last_fetch / TSTAGES) & 1);
+    if (last_fetch >= 0) tc::mbar_wait(&tma_bar[last_fetch % S::TSTAGES], uint32_t(last_fetch / S::TSTAGES) & 1);
     if (last_commit >= 0) tc::mbar_wait(&mma_bar[last_commit & 1], uint32_t(last_commit >> 1) & 1);
   }
   tc::tc_fence_before();

@@ -188,7 +188,7 @@ struct EnergyParts {
 struct Tuning {
   int ksplit = 4096;       // particles per split-K chunk of a box in the outgoing pass
   int ksplit_root = 2048;  // particles per chunk of the root pass
-  int inc_waves = 4;       // resident waves of blocks (8 per SM) in the incoming pass
+  int inc_waves = 4;       // resident waves of blocks (3 per SM) in the incoming pass
   int res_ny_max = 8;      // most target chunks (64 targets each) per leaf in the near field
 };
 
@@ -310,8 +310,8 @@ class DmkTree {
   int n_nonleaf_ = 0, n_leaves_ = 0;
   int* d_nonleaf_ = nullptr;  // non-leaf nodes of the expansion levels
   int* d_leaves_ = nullptr;   // leaves at levels >= 2
-  int n_groups_ = 0;
-  int* d_groups_ = nullptr;   // parents of expansion boxes with a non-leaf child
+  int n_cubes_ = 0;
+  int* d_cubes_ = nullptr;    // boxes two levels above the expansion levels with a non-leaf grandchild
   double* d_Cl_ = nullptr;
   double* d_Sl_ = nullptr;
   double* d_scalars_ = nullptr;
