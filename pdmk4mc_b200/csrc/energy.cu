@@ -366,8 +366,10 @@ __device__ inline int refined_rank(const DevTree& T, int level, uint64_t cell) {
 // slot + slots, ... of cube c, so its set-up (the cube's cell lookup) is
 // paid once, and the cubes sharing a slot walk the same tiles together (the
 // cells two neighbouring cubes share meet in L2).
-__global__ void __launch_bounds__(INC_T, 3) k_incoming_cube(DevTree T, const int* __restrict__ cubes, int ncubes,
-                                                          int slots, double* part) {
+template <int NK>
+__global__ void __launch_bounds__(INC_T, 2) k_incoming_cube(DevTree T, const int* __restrict__ cubes, int ncubes,
+                                                             int slots, double* part) {
+  constexpr int D = 2 * NK + 1, H = (NK + 1) * D * D;
   extern __shared__ double2 w[];                             // [INC_CELLS][INC_KT]
   int* s_row = reinterpret_cast<int*>(w + INC_CELLS * INC_KT);  // outgoing row of each cell, -1: absent or empty
   int* s_recv = s_row + INC_CELLS;                           // expansion row of each receiver, -1: none
@@ -385,6 +387,7 @@ __global__ void __launch_bounds__(INC_T, 3) k_incoming_cube(DevTree T, const int
     const int c[3] = {t % 6 - 1, (t / 6) % 6 - 1, t / 36 - 1};
     int g[3];
     unsigned wrap = 0;
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
       int v = O[a] + c[a];
       const int f = v < 0 ? 1 : (v >= side ? 2 : 0);  // 1: image below (-1), 2: above (+1)
@@ -402,32 +405,56 @@ __global__ void __launch_bounds__(INC_T, 3) k_incoming_cube(DevTree T, const int
       s_recv[c[0] + 4 * c[1] + 16 * c[2]] = (node >= 0 && T.node_child0[node] >= 0) ? node - base : -1;
   }
   __syncthreads();
-  const int n = T.n_diff, d = T.dd;
   const int two_l = (l & 1) ? 2 : 1;
   const int kk = threadIdx.x % INC_KT;
   const int line = threadIdx.x / INC_KT, ry = line & 3, rz = line >> 2;
+  const double2 w3a = make_double2(-0.5, -0.86602540378443864676);  // exp(-2 pi i / 3)
+  const double2 w3b = make_double2(-0.5, 0.86602540378443864676);   // exp(-4 pi i / 3)
   double e = 0;
-  const int ktiles = (T.H + INC_KT - 1) / INC_KT;
+  constexpr int ktiles = (H + INC_KT - 1) / INC_KT;
   for (int tile = slot; tile < ktiles; tile += slots) {
     const int k = tile * INC_KT + kk;
-    const bool kin = k < T.H;
-    const int ix = k % d, iy = (k / d) % d, iz = k / (d * d);
-    const int a[3] = {((ix - n) % 3 + 3) % 3, ((iy - n) % 3 + 3) % 3, ((iz - n) % 3 + 3) % 3};
-    // stage the cube: mode kk of cells line, line + 16, ...
-    for (int c = line; c < INC_CELLS; c += INC_T / INC_KT) {
-      const int row = s_row[c];
-      double2 v = (row >= 0 && kin) ? T.out[size_t(row) * T.H + k] : make_double2(0.0, 0.0);
+    const bool kin = k < H;
+    const int ix = k % D, iy = (k / D) % D, iz = k / (D * D);
+    // the image phase is exp(-2 pi i e / 3) with e = sum over axes of
+    // f (i - n) 2^l mod 3 (f = -1 below, +1 above): per axis the terms of
+    // an image below and above, two bits each
+    unsigned below = 0, above = 0;
+    {
+      const int ii[3] = {ix, iy, iz};
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        const int b = (((ii[ax] - NK) % 3 + 3) * two_l) % 3;
+        above |= unsigned(b) << (2 * ax);
+        below |= unsigned((3 - b) % 3) << (2 * ax);
+      }
+    }
+    // stage the cube: mode kk of cells line, line + 16, ...; all loads issued
+    // before the first is used
+    constexpr int NPT = (INC_CELLS + INC_T / INC_KT - 1) / (INC_T / INC_KT);  // cells per thread
+    double2 vv[NPT];
+#pragma unroll
+    for (int i = 0; i < NPT; ++i) {
+      const int c = line + i * (INC_T / INC_KT);
+      const int row = c < INC_CELLS ? s_row[c] : -1;
+      vv[i] = (row >= 0 && kin) ? T.out[size_t(row) * H + k] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int i = 0; i < NPT; ++i) {
+      const int c = line + i * (INC_T / INC_KT);
+      if (c >= INC_CELLS) break;
+      double2 v = vv[i];
       const unsigned wr = s_wrap[c];
       if (wr) {
-        // image phase exp(-i 2 pi sgn / 3) = w6^{-2 sgn}, sgn = (k - n).f 2^l;
-        // the sum lies in [-12, 12]
-        int sg = 0;
+        unsigned ep = 0;
+#pragma unroll
         for (int ax = 0; ax < 3; ++ax) {
           const unsigned f = (wr >> (2 * ax)) & 3u;
-          sg += f == 1 ? -a[ax] : (f == 2 ? a[ax] : 0);
+          ep += f == 1 ? (below >> (2 * ax)) & 3u : (f == 2 ? (above >> (2 * ax)) & 3u : 0u);
         }
-        const int e3 = (sg * two_l + 12) % 3;
-        if (e3) v = cmul(v, root6(-2 * e3));
+        ep = ep >= 3 ? ep - 3 : ep;
+        ep = ep >= 3 ? ep - 3 : ep;
+        if (ep) v = cmul(v, ep == 1 ? w3a : w3b);
       }
       w[c * INC_KT + kk] = v;
     }
@@ -444,20 +471,42 @@ __global__ void __launch_bounds__(INC_T, 3) k_incoming_cube(DevTree T, const int
       col[cx] = acc;
     }
     if (kin) {
+      const double d2 = T.D2[k];
 #pragma unroll
       for (int x = 0; x < 4; ++x) {
         const int rrow = s_recv[x + 4 * ry + 16 * rz];
         if (rrow < 0) continue;
         const double2 inc = cconj(cadd(cadd(col[x], col[x + 1]), col[x + 2]));
-        T.inc[size_t(rrow) * T.H + k] = inc;
+        T.inc[size_t(rrow) * H + k] = inc;
         const double2 o = w[((rz + 1) * 36 + (ry + 1) * 6 + x + 1) * INC_KT + kk];  // the receiver's own row
-        e += (o.x * inc.x - o.y * inc.y) * T.D2[k];
+        e += (o.x * inc.x - o.y * inc.y) * d2;
       }
     }
     __syncthreads();
   }
   double s = block_sum(e, sm);
   if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+template <int NK>
+void launch_incoming_nk(const DevTree& D, const int* cubes, int ncubes, int slots, double* part, cudaStream_t st) {
+  raise_smem_limit(reinterpret_cast<const void*>(k_incoming_cube<NK>), INC_SMEM);
+  k_incoming_cube<NK><<<unsigned(slots * ncubes), INC_T, INC_SMEM, st>>>(D, cubes, ncubes, slots, part);
+  PDMK_LAUNCH_CHECK();
+}
+
+void launch_incoming(const DevTree& D, const int* cubes, int ncubes, int slots, double* part, cudaStream_t st) {
+  switch (D.n_diff) {
+    case 4: launch_incoming_nk<4>(D, cubes, ncubes, slots, part, st); break;
+    case 6: launch_incoming_nk<6>(D, cubes, ncubes, slots, part, st); break;
+    case 8: launch_incoming_nk<8>(D, cubes, ncubes, slots, part, st); break;
+    case 12: launch_incoming_nk<12>(D, cubes, ncubes, slots, part, st); break;
+    case 13: launch_incoming_nk<13>(D, cubes, ncubes, slots, part, st); break;
+    case 17: launch_incoming_nk<17>(D, cubes, ncubes, slots, part, st); break;
+    case 19: launch_incoming_nk<19>(D, cubes, ncubes, slots, part, st); break;
+    case 26: launch_incoming_nk<26>(D, cubes, ncubes, slots, part, st); break;
+    default: throw std::invalid_argument("incoming pass: unsupported mode count");
+  }
 }
 
 // E_diff from the cube-tiled partials: sum over cubes C_l dscale_l
@@ -1240,16 +1289,12 @@ void DmkTree::run_incoming(bool write_inc) {
   k_box_q2<<<unsigned(n_nonleaf_), TPB, 0, st_>>>(D, d_nonleaf_, q2);
   PDMK_LAUNCH_CHECK();
   if (write_inc) {
-    // about inc_waves resident waves of blocks (three per SM), each walking a
+    // about inc_waves resident waves of blocks (two per SM), each walking a
     // strided set of tiles
     const int kt = (D.H + INC_KT - 1) / INC_KT;
     const int nc = std::max(n_cubes_, 1);
-    const int slots = std::max(1, std::min(kt, (tune_.inc_waves * 3 * 148 + nc - 1) / nc));
-    if (n_cubes_ > 0) {
-      raise_smem_limit(reinterpret_cast<const void*>(k_incoming_cube), INC_SMEM);
-      k_incoming_cube<<<unsigned(slots * n_cubes_), INC_T, INC_SMEM, st_>>>(D, d_cubes_, n_cubes_, slots, part);
-      PDMK_LAUNCH_CHECK();
-    }
+    const int slots = std::max(1, std::min(kt, (tune_.inc_waves * 2 * 148 + nc - 1) / nc));
+    if (n_cubes_ > 0) launch_incoming(D, d_cubes_, n_cubes_, slots, part, st_);
     k_diff_finish_cube<<<1, 1024, 0, st_>>>(D, d_cubes_, n_cubes_, slots, part, d_nonleaf_, n_nonleaf_, q2, d_Cl_,
                                             d_Sl_, d_scalars_ + 1);
     PDMK_LAUNCH_CHECK();

@@ -188,7 +188,7 @@ struct EnergyParts {
 struct Tuning {
   int ksplit = 4096;       // particles per split-K chunk of a box in the outgoing pass
   int ksplit_root = 2048;  // particles per chunk of the root pass
-  int inc_waves = 4;       // resident waves of blocks (3 per SM) in the incoming pass
+  int inc_waves = 4;       // resident waves of blocks (2 per SM) in the incoming pass
   int res_ny_max = 8;      // most target chunks (64 targets each) per leaf in the near field
 };
 
