@@ -416,6 +416,8 @@ def run_b200(args, rank, ws):
         timing = mixed.tree.get_timing()
         mixed.tree.set_timing(False)
     res = {k: a.summary(ws, ew_uniform) for k, a in arms.items()}
+    # the run-time splits and tiles the trees took from the autotuner's table
+    tuning = {k: a.tree.tuning() for k, a in arms.items()}
     M = W["moves_per_step"]
     steps_time = sum(float(np.sum(a.t_moves) + np.sum(a.t_energy) + np.sum(a.t_cand)) for a in arms.values())
 
@@ -541,6 +543,8 @@ def run_b200(args, rank, ws):
                     "full_energy_h2d_bytes": n * 32, "full_energy_d2h_bytes": 8,
                     "path": "mixed precision through hpdmk_mc_run and hpdmk_tree_init + outgoing + incoming + "
                             "energy with host arrays"},
+            "tuning": dict(tuning, source="pdmk4mc_b200/tuning.json (hpdmk_autotune), looked up per "
+                                          "(digits, precision, floor(log2 N))"),
             "gpu_launches": int(launches),
             "clocks": c,
         }
@@ -578,6 +582,17 @@ def run_profile(args):
         idx, disp, u = make_moves(1, W["N"], M, W["step"])
         t.mc_run(idx, disp, u, W["beta"])
         t.close()
+    if args.single_moves > 0:
+        # single-move energy shifts and accepted updates (hpdmk_eval_shift_energy,
+        # hpdmk_update_shift), each its own launch
+        t = P.HPDMKPtTree(params, r, q, leaf_slack=8, precision=prec)
+        t.form_outgoing_pw()
+        t.form_incoming_pw()
+        idx, disp, _ = make_moves(2, W["N"], args.single_moves, W["step"])
+        for i, d in zip(idx, disp):
+            t.eval_shift_energy(int(i), *d)
+            t.update_shift(int(i), *d)
+        t.close()
     print(f"profile run done: {args.profile} {args.precision} E={e!r}")
 
 
@@ -594,6 +609,8 @@ def main():
                     help="a short run for profilers on one workload (prints no bench line)")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--single-moves", type=int, default=0,
+                    help="--profile only: this many single-move shifts and updates after the Metropolis run")
     ap.add_argument("--mc-graph", action="store_true",
                     help="profile runs: Metropolis moves as graphs of (k_shift, k_update) launches")
     args = ap.parse_args()
