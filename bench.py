@@ -30,6 +30,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import re
 import os
 import subprocess
 import sys
@@ -430,9 +431,12 @@ def run_b200(args, rank, ws):
     bytes_per_launch = (mixed.work[1] + mixed.work[2]) / max(mc_n, 1)
     achieved = bytes_per_launch / (mc_ms / mc_n / 1e3) / 1e9 if mc_n else None
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "k_mc_traffic_uniform_n1e6_d9.json")
+    # DRAM bytes per move from the ncu capture summarised in the k_mc profile
+    tpath = os.path.join(ROOT, "profiles", "k_mc_uniform_n1e5_d9.md")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath))["dram_bytes_per_move"] * M
+        mt = re.search(r"^dram_bytes_per_move = (\d+)", open(tpath).read(), re.M)
+        if mt:
+            traffic = int(mt.group(1)) * M
 
     # end to end through the C-ABI with host buffers, mixed path: the moves
     # (hpdmk_mc_run: indices, displacements and uniforms in, shifts and
@@ -532,7 +536,8 @@ def run_b200(args, rank, ws):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 256-move k_mc "
-                                           "launch on this workload, scaled by moves per launch" if traffic else None,
+                                           "launch on this workload, scaled by moves per launch "
+                                           "(profiles/k_mc_uniform_n1e5_d9.md)" if traffic else None,
                          "kernel": f"k_mc (persistent Metropolis, mixed arm: dE reads + accept-and-update "
                                    f"read-modify-writes, {M} moves per launch)",
                          "timed_launches": int(mc_n), "peak_source": peak_kind},
