@@ -18,6 +18,7 @@
 #include <stdexcept>
 
 #include "common.cuh"
+#include "hostpar.hpp"
 #include "sort.cuh"
 #include "tree.hpp"
 
@@ -502,8 +503,7 @@ void DmkTree::build(const double* r_in, const double* q_in, bool on_device) {
     PDMK_CUDA(cudaMallocAsync(&tmp_in, size_t(4 * n) * sizeof(double), st_));
     r = static_cast<double*>(tmp_in);
     q = r + 3 * n;
-    PDMK_CUDA(cudaMemcpyAsync(r, r_in, size_t(3 * n) * sizeof(double), cudaMemcpyHostToDevice, st_));
-    PDMK_CUDA(cudaMemcpyAsync(q, q_in, size_t(n) * sizeof(double), cudaMemcpyHostToDevice, st_));
+    staged_h2d(r, {{r_in, size_t(3 * n) * sizeof(double)}, {q_in, size_t(n) * sizeof(double)}}, st_);
   }
   // refined cells per level (level 0: the root) and, in the last word, the
   // count of invalid device inputs; read back together after the shallow
@@ -1137,6 +1137,52 @@ void DmkTree::export_D(int level, double* out) const {
   PDMK_CUDA(cudaMemcpyAsync(out, dev_.D2, sizeof(double) * dev_.H, cudaMemcpyDeviceToHost, st_));
   PDMK_CUDA(cudaStreamSynchronize(st_));
   for (int k = 0; k < dev_.H; ++k) out[k] *= dev_.dscale[level];
+}
+
+namespace {
+struct Staging {
+  std::mutex mu;
+  char* buf = nullptr;
+  size_t cap = 0;
+  cudaEvent_t done = nullptr;  // the last copy out of buf
+};
+Staging g_staging[64];
+}  // namespace
+
+void staged_h2d(void* dst, const std::vector<HostPiece>& pieces, cudaStream_t st) {
+  size_t total = 0;
+  for (const HostPiece& p : pieces) total += p.bytes;
+  int dev = 0;
+  PDMK_CUDA(cudaGetDevice(&dev));
+  if (total < (size_t(4) << 20) || dev < 0 || dev >= 64) {
+    char* d = static_cast<char*>(dst);
+    for (const HostPiece& p : pieces) {
+      PDMK_CUDA(cudaMemcpyAsync(d, p.src, p.bytes, cudaMemcpyHostToDevice, st));
+      d += p.bytes;
+    }
+    return;
+  }
+  Staging& S = g_staging[dev];
+  std::lock_guard<std::mutex> g(S.mu);
+  if (S.done) PDMK_CUDA(cudaEventSynchronize(S.done));
+  else PDMK_CUDA(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming));
+  if (S.cap < total) {
+    if (S.buf) PDMK_CUDA(cudaFreeHost(S.buf));
+    S.buf = nullptr;
+    S.cap = 0;
+    PDMK_CUDA(cudaMallocHost(reinterpret_cast<void**>(&S.buf), total));
+    S.cap = total;
+  }
+  size_t off = 0;
+  for (const HostPiece& p : pieces) {
+    const char* src = static_cast<const char*>(p.src);
+    char* stage = S.buf + off;
+    parallel_chunks(long(p.bytes),
+                    [&](long b, long e) { std::memcpy(stage + b, src + b, size_t(e - b)); }, 1L << 22);
+    off += p.bytes;
+  }
+  PDMK_CUDA(cudaMemcpyAsync(dst, S.buf, total, cudaMemcpyHostToDevice, st));
+  PDMK_CUDA(cudaEventRecord(S.done, st));
 }
 
 }  // namespace pdmk

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/hpdmk.h"
+#include "hostpar.hpp"
 #include "tree.hpp"
 
 namespace pdmk {
@@ -142,10 +143,20 @@ int check_params(const HPDMKParams& p) {
 
 int check_inputs(double L, int n, const double* r, const double* q) {
   if (n < 1 || !r || !q) return fail(HPDMK_ERR_BAD_INPUT, "need n >= 1 particles with positions and charges");
-  for (long k = 0; k < 3L * n; ++k)
-    if (!(r[k] >= 0.0 && r[k] < L)) return fail(HPDMK_ERR_BAD_INPUT, "positions must lie in [0, L)");
-  for (long k = 0; k < n; ++k)
-    if (!std::isfinite(q[k])) return fail(HPDMK_ERR_BAD_INPUT, "charges must be finite");
+  // branch-free scans over pieces of the arrays, on a few threads
+  std::atomic<int> bad_r{0}, bad_q{0};
+  pdmk::parallel_chunks(3L * n, [&](long b, long e) {
+    int bad = 0;
+    for (long k = b; k < e; ++k) bad |= !(r[k] >= 0.0 && r[k] < L);
+    if (bad) bad_r = 1;
+  });
+  pdmk::parallel_chunks(long(n), [&](long b, long e) {
+    int bad = 0;
+    for (long k = b; k < e; ++k) bad |= !std::isfinite(q[k]);
+    if (bad) bad_q = 1;
+  });
+  if (bad_r) return fail(HPDMK_ERR_BAD_INPUT, "positions must lie in [0, L)");
+  if (bad_q) return fail(HPDMK_ERR_BAD_INPUT, "charges must be finite");
   return HPDMK_OK;
 }
 

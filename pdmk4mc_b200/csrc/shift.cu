@@ -326,6 +326,25 @@ __device__ inline void block_sum4(double* v, double (*sm)[32]) {
   __syncthreads();
 }
 
+// as block_sum4, the sums in thread 0 only and no barrier after them (the
+// caller's next barrier orders its use)
+__device__ inline void block_sum4_t0(double* v, double (*sm)[32]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
+  __syncthreads();
+  if (lane == 0)
+    for (int c = 0; c < 4; ++c) sm[c][warp] = v[c];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 4; ++c) {
+      double s = 0;
+      for (int w = 0; w < nw; ++w) s += sm[c][w];
+      v[c] = s;
+    }
+}
+
 // slot s of a path level: 0 own outgoing, 1 own incoming, 2.. the colleague
 // in direction dir (dir != 13, dx fastest)
 __device__ inline int slot_of_dir(int dir) { return 2 + (dir < 13 ? dir : dir - 1); }
@@ -852,7 +871,8 @@ __device__ bool mc_barrier(const DevTree& T, const McArgs& a, unsigned& nbar) {
       }
       __nanosleep(32);
     }
-    __threadfence();
+    // the acquire load above orders this thread after the other blocks'
+    // releases; the barrier below passes that order on to the whole block
     s_ok = ok;
   }
   __syncthreads();
@@ -1076,16 +1096,21 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
       acc[3] *= h.q;
     }
     const int s_next = threadIdx.x < 32 ? __ldcg(T.orig_slot + i_next) : 0;
-    block_sum4(acc, red);
+    block_sum4_t0(acc, red);
     double* part = a.partials + size_t(m & 1) * 4 * G;
     if (threadIdx.x == 0)
       for (int c = 0; c < 4; ++c) part[4 * blockIdx.x + c] = acc[c];
     if (!mc_barrier(T, a, nbar)) return;
-    // every block reduces the same partials in the same order
+    // every block reduces the same partials in the same order: one warp,
+    // lane-strided sums then a shuffle tree into lane 0
     double tot[4] = {0, 0, 0, 0};
-    for (int b = threadIdx.x; b < G; b += blockDim.x)
-      for (int c = 0; c < 4; ++c) tot[c] += __ldcg(part + 4 * b + c);
-    block_sum4(tot, red);
+    if (threadIdx.x < 32) {
+      for (int b = threadIdx.x; b < G; b += 32)
+        for (int c = 0; c < 4; ++c) tot[c] += __ldcg(part + 4 * b + c);
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        for (int o = 16; o > 0; o >>= 1) tot[c] += __shfl_down_sync(0xffffffffu, tot[c], o);
+    }
     if (threadIdx.x == 0) {
       const double dEw = tot[0] * a.c_window;
       double self = 0;
