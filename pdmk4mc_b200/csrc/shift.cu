@@ -845,18 +845,25 @@ __device__ inline unsigned ld_acquire(const unsigned* p) {
   return v;
 }
 
-// Grid barrier over a monotonically increasing arrival counter; nbar counts
-// the barriers this block has passed (kept by thread 0). False when the wait
-// gave up or another block reported a failure.
-__device__ bool mc_barrier(const DevTree& T, const McArgs& a, unsigned& nbar) {
-  __shared__ int s_ok;
+// Grid barrier over a monotonically increasing arrival counter, as an
+// arrival and a wait that may be apart; nbar counts the barriers this block
+// has arrived at (kept by thread 0).
+__device__ void mc_arrive(const McArgs& a, unsigned& nbar) {
   __syncthreads();
   if (threadIdx.x == 0) {
     ++nbar;
-    const unsigned target = nbar * gridDim.x;
     // the release orders this block's writes (made visible to this thread by
     // the __syncthreads above) before the arrival; no reply is awaited
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(a.arrivals) : "memory");
+  }
+}
+
+// Waits until every block has arrived at this block's last barrier. False
+// when the wait gave up or another block reported a failure.
+__device__ bool mc_wait(const DevTree& T, const McArgs& a, unsigned nbar) {
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    const unsigned target = nbar * gridDim.x;
     int ok = 1;
     for (long long it = 0;; ++it) {
       if (ld_acquire(a.arrivals) >= target) break;
@@ -877,6 +884,11 @@ __device__ bool mc_barrier(const DevTree& T, const McArgs& a, unsigned& nbar) {
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+__device__ bool mc_barrier(const DevTree& T, const McArgs& a, unsigned& nbar) {
+  mc_arrive(a, nbar);
+  return mc_wait(T, a, nbar);
 }
 
 // Source lists of one path's leaf for the near field: the leaf, its 26
@@ -927,6 +939,7 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
   __shared__ int s_acc;
   __shared__ int s_rounds[9];  // grid-stride rounds of H*g update units
   __shared__ int s_pn;         // overflow pool fill
+  __shared__ int s_stale;      // the accepted move invalidated the preloaded next particle
   const ResidualPoly<NP> poly(T);
   if (threadIdx.x >= 1 && threadIdx.x <= 8) {
     const long units = long(T.H) * threadIdx.x, gs = long(gridDim.x) * blockDim.x;
@@ -952,12 +965,23 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
   if (threadIdx.x < 32)
     for (int c = 0; c < 3; ++c) d_cur[c] = a.disp[c];
   Preload pre{-1, 0, 0, 0, 0};
+  // An accepted move ends with an arrival at a grid barrier whose wait is
+  // deferred: the next move's resolve and phase tables read only the
+  // preloaded particle and the static refinement bitmaps, so they run before
+  // the wait; the near-field source lists, the pool fill and the sums, which
+  // read what other blocks update or commit, run after it. When the accepted
+  // move invalidated the preload, the wait comes first.
+  bool pend = false;
   for (int m = 0; m < a.n_moves; ++m) {
     const bool more = threadIdx.x < 32 && m + 1 < a.n_moves;
     const int i_next = more ? a.idx[m + 1] : 0;
     double d_next[3] = {0, 0, 0};
     if (more)
       for (int c = 0; c < 3; ++c) d_next[c] = a.disp[3 * (m + 1) + c];
+    if (pend && s_stale) {
+      if (!mc_wait(T, a, nbar)) return;
+      pend = false;
+    }
     resolve<true>(T, i_cur, d_cur, h, &pre);
     const int lo_max = h.depth_o - 2, lt_max = h.depth_t - 2;
     // the incoming rows of both paths go to L2 while the tables are built
@@ -973,15 +997,23 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
     alloc_tables(sm2, T, oo);
     alloc_tables(sm2 + per, T, to);
     // near-field source lists on threads 0..71, phase tables on the rest
-    if (threadIdx.x < 72) {
+    auto source_lists = [&]() {
       if (threadIdx.x == 0) s_pn = __ldcg(T.pool_n);
       const int p = threadIdx.x / 36, src = threadIdx.x % 36;
       const int lv = (p == 0 ? h.depth_t : h.depth_o) - 1;
       res_meta(T, p == 0 ? h.path_t[lv] : h.path_o[lv], lv, p == 0 ? h.Xt[lv] : h.Xo[lv], src, meta[p]);
+    };
+    if (threadIdx.x < 72) {
+      if (!pend) source_lists();
     } else {
       const int nthr = blockDim.x - 72, t = threadIdx.x - 72;
       build_tables(T, h.xo, h.q, h.Xo, uo, oo, t, nthr);
       build_tables(T, h.xt, h.q, h.Xt, ut, to, t, nthr);
+    }
+    if (pend) {
+      if (!mc_wait(T, a, nbar)) return;
+      pend = false;
+      if (threadIdx.x < 72) source_lists();
     }
     __syncthreads();
     if (threadIdx.x < 2) {
@@ -1134,6 +1166,7 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
       // (its own slot and the slot of the particle swapped into its place) or
       // moved that very particle
       const bool stale = s_acc && (h.path_o[h.depth_o - 1] != h.path_t[h.depth_t - 1] || i_next == h.i_orig);
+      if (threadIdx.x == 0) s_stale = stale;
       // a kept slot is loaded now; an accepted move writes other slots only,
       // and the commit of a same-leaf move of this very particle marks it stale
       pre.s = -1;
@@ -1252,7 +1285,8 @@ __global__ void __launch_bounds__(MC_T, 1) k_mc(DevTree T, McArgs a) {
         }
       }
     }
-    if (!mc_barrier(T, a, nbar)) return;
+    mc_arrive(a, nbar);
+    pend = true;
   }
 }
 
