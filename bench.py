@@ -64,6 +64,57 @@ def make_system(seed, n, L):
     return r, q
 
 
+REPLICAS = dict(workload="256 replicas, N log-uniform in [2e3, 5e4] (even), L = N^(1/3), n_per_leaf = N / 128",
+                n_replicas=256, n_min=2000, n_max=50000, digits=9, moves_per_replica=64, step=0.3, beta=1.0,
+                charges="alternating +1/-1", precision="mixed")
+
+
+def run_replicas(P, torch, seed=11, steps=3, warmup=2):
+    """Replica sets: the trees' full energies (outgoing, incoming, energy of
+    the built trees, several in flight: hpdmk_replicas_energy) and their
+    Metropolis sequences in one launch (hpdmk_replicas_mc_run); wall clock on
+    the host around the synchronous calls, aggregate rates."""
+    R = REPLICAS
+    rng = np.random.default_rng(seed)
+    ns = (np.rint(np.exp(rng.uniform(np.log(R["n_min"]), np.log(R["n_max"]), R["n_replicas"]))) // 2 * 2).astype(int)
+    trees = []
+    try:
+        for k, n in enumerate(ns):
+            L = float(n) ** (1.0 / 3.0)
+            r = rng.uniform(0.0, L, 3 * n)
+            q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+            prm = P.HPDMKParams(n_per_leaf=max(8, int(n) // 128), digits=R["digits"], L=L, init=P.DIRECT)
+            trees.append(P.HPDMKPtTree(prm, r, q, leaf_slack=8, precision=P.PRECISION_MIXED))
+        m = R["moves_per_replica"]
+        te, tm = [], []
+        for s in range(warmup + steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            P.replicas_energy(trees)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            idx = np.stack([rng.integers(0, n, m) for n in ns])
+            disp = rng.uniform(-R["step"], R["step"], (len(ns), m, 3))
+            u = rng.uniform(0, 1, (len(ns), m))
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            _, acc = P.replicas_mc_run(trees, idx, disp, u, R["beta"])
+            torch.cuda.synchronize()
+            t3 = time.perf_counter()
+            if s >= warmup:
+                te.append(t1 - t0)
+                tm.append(t3 - t2)
+        return {"full_energies_per_s": len(ns) * steps / sum(te), "energy_set_ms": 1e3 * sum(te) / steps,
+                "moves_per_s": len(ns) * m * steps / sum(tm), "move_set_ms": 1e3 * sum(tm) / steps,
+                "particles": int(ns.sum()), "n_min": int(ns.min()), "n_max": int(ns.max()),
+                "timing": "host wall clock around the synchronous calls",
+                "energy": "outgoing + incoming + energy of the built trees (hpdmk_replicas_energy)",
+                "config": dict(R, steps=steps, warmup=warmup)}
+    finally:
+        for t in trees:
+            t.close()
+
+
 def make_clustered(seed, n, L, n_clusters=64, frac=0.8):
     rng = np.random.default_rng(seed)
     m = int(frac * n)
@@ -485,6 +536,10 @@ def run_b200(args, rank, ws):
                                   "moves": clustered["mixed"]["moves_per_s"] / clustered["fp64"]["moves_per_s"]}
     clustered["config"] = dict(CLUSTERED, steps=cargs.steps)
 
+    # replica sets (config 4), mixed precision
+    replicas = run_replicas(P, torch) if ws == 1 else None
+    torch.cuda.empty_cache()
+
     # the N = 1e5 cube, against the stored CPU Ewald energy
     W5 = dict(WORKLOAD_N1E5)
     r5, q5 = make_system(1, W5["N"], W5["L"])
@@ -533,6 +588,7 @@ def run_b200(args, rank, ws):
                                   "to 1e-10 by the tests"},
             "clustered": clustered,
             "n1e5": n1e5,
+            "replicas": replicas,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 256-move k_mc "

@@ -74,11 +74,12 @@ typedef void *hpdmk_tree;
  * HPDMK_PRECISION_FP64: every step in FP64 (the drop-in path).
  * HPDMK_PRECISION_MIXED: the outgoing plane-wave expansions (root and boxes,
  * the reference's outgoing_pw_root / outgoing_pw_direct, src/planewave.cpp:24-84)
- * are formed on the tensor cores from 8-bit integer slices of the phase
- * factors (three 7-bit slices per operand, exact 32-bit integer sums,
- * FP64 combination), a coefficient error near 1e-7 of the largest factor;
- * the incoming expansions, energy sums, near field, energy shifts and updates
- * stay FP64. */
+ * are formed on the tensor cores (tcgen05, kind::i8) from 8-bit slices: each
+ * operand is a 32-bit fixed point written as four signed base-256 digits, the
+ * ten slice products of order <= 3 are summed exactly in 32-bit integers and
+ * combined in FP64, a coefficient error near 1e-9 of the box's largest
+ * coefficient (energies within about 1e-9 of the FP64 path); the incoming
+ * expansions, energy sums, near field, energy shifts and updates stay FP64. */
 #define HPDMK_PRECISION_FP64 0
 #define HPDMK_PRECISION_MIXED 1
 
@@ -215,6 +216,24 @@ int hpdmk_eval_potential(hpdmk_tree tree, int m, const long *i, double *phi, dou
  * particles' original indices stay; the result equals a tree built from
  * hpdmk_get_positions. Runs on the device. */
 int hpdmk_tree_rebuild(hpdmk_tree tree);
+
+/* Rebuild policy: with leaf_factor > 1, every hpdmk_form_outgoing_pw first
+ * checks how far the tree has drifted from the refinement rule under the
+ * accepted moves and rebuilds it (as hpdmk_tree_rebuild, before forming the
+ * outgoing expansions) when a leaf holds more than leaf_factor * n_per_leaf
+ * particles or a refined node below level 2 holds fewer than
+ * n_per_leaf / leaf_factor. Both thresholds are widened to the tree's own
+ * values when the policy was set or the tree last rebuilt (leaves at the
+ * level cap may hold more than n_per_leaf, nodes refined for the 2:1 balance
+ * fewer), so a tree as built never triggers it. leaf_factor = 0 (the
+ * default) turns the check off. The check is one small kernel and one
+ * read-back per full energy. */
+int hpdmk_set_rebuild_policy(hpdmk_tree tree, double leaf_factor);
+
+/* The drift the policy looks at: the largest particle count of a leaf and
+ * the smallest of a refined node below level 2 (n if there is none), from
+ * the counts the moves maintain; *rebuilds = rebuilds the policy made. */
+int hpdmk_tree_drift(hpdmk_tree tree, int *max_leaf, int *min_refined, int *rebuilds);
 
 /* FP64 Ewald energy of the current particles, the comparator for the DMK
  * energy (reference: the Ewald summation of src/ewald.cpp:17-223, there on

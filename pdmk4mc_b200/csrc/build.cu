@@ -1072,6 +1072,45 @@ __global__ void k_gather_orig(int n, const int* orig_slot, int n_slots, const do
 }
 }  // namespace
 
+namespace {
+// out[0] = max count over leaves, out[1] = min count over refined nodes of
+// levels >= 3 (refinement above is forced)
+__global__ void k_drift(const int* __restrict__ count, const int* __restrict__ child0, const int* __restrict__ level,
+                        int n_nodes, int* out) {
+  int mx = 0, mn = 0x7fffffff;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes; i += gridDim.x * blockDim.x) {
+    const int c = count[i];
+    if (child0[i] < 0) mx = max(mx, c);
+    else if (level[i] >= 3) mn = min(mn, c);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, mx);
+    atomicMin(out + 1, mn);
+  }
+}
+}  // namespace
+
+void DmkTree::drift(int* max_leaf, int* min_refined) const {
+  const DevTree& D = dev_;
+  int* d_out = nullptr;
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_out), 2 * sizeof(int), st_));
+  const int init[2] = {0, int(N_)};
+  PDMK_CUDA(cudaMemcpyAsync(d_out, init, sizeof(init), cudaMemcpyHostToDevice, st_));
+  const int blocks = std::max(1, std::min(592, (D.n_nodes + 255) / 256));
+  k_drift<<<unsigned(blocks), 256, 0, st_>>>(D.node_count, D.node_child0, D.node_level, D.n_nodes, d_out);
+  PDMK_LAUNCH_CHECK();
+  int out[2];
+  PDMK_CUDA(cudaMemcpyAsync(out, d_out, sizeof(out), cudaMemcpyDeviceToHost, st_));
+  PDMK_CUDA(cudaFreeAsync(d_out, st_));
+  PDMK_CUDA(cudaStreamSynchronize(st_));
+  *max_leaf = out[0];
+  *min_refined = out[1];
+}
+
 void DmkTree::gather_device(double* d_r, double* d_q) const {
   const DevTree& D = dev_;
   const int n = int(N_);

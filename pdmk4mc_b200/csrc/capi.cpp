@@ -4,6 +4,7 @@
 // include/utils.hpp:47, src/upward_pass.cpp:13).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -37,6 +38,9 @@ struct Handle {
   long n = 0;
   double L = 0;
   int device = 0;
+  double rebuild_factor = 0;  // rebuild policy: 0 off, else the leaf drift factor
+  int rebuilds = 0;           // rebuilds the policy made
+  int base_max = 0, base_min = 0;  // the drift of the tree when the policy was set or last rebuilt
   // staging buffers for the host-array batched calls
   int* d_i = nullptr;
   double* d_d = nullptr;
@@ -123,6 +127,34 @@ struct DeviceGuard {
   DeviceGuard(const DeviceGuard&) = delete;
   DeviceGuard& operator=(const DeviceGuard&) = delete;
 };
+
+// Re-bins the tree from its particles' current positions on the device: a
+// fresh tree of the same parameters, settings and tuning replaces the old
+// one (the expansions are not formed here).
+void rebuild_structure(Handle* h) {
+  const pdmk::DmkTree& old = *h->tree;
+  const long n = old.n_particles();
+  double* d_r = nullptr;
+  PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_r), sizeof(double) * 4 * size_t(n), h->stream));
+  double* d_q = d_r + 3 * n;
+  old.gather_device(d_r, d_q);
+  try {
+    auto nt = std::make_unique<pdmk::DmkTree>(old.box(), old.n_per_leaf(), old.digits(), n, d_r, d_q, true,
+                                              old.options(), h->stream);
+    nt->set_mc_mode(old.mc_mode());  // the caller's settings carry over
+    nt->set_tuning(old.tuning());
+    h->tree = std::move(nt);
+  } catch (...) {
+    cudaFreeAsync(d_r, h->stream);
+    throw;
+  }
+  PDMK_CUDA(cudaFreeAsync(d_r, h->stream));
+}
+
+// The drift of a tree as built is the policy's baseline: leaves at the level
+// cap may hold more than n_per_leaf particles and nodes refined for the 2:1
+// balance fewer, and neither is drift.
+void record_baseline(Handle* h) { h->tree->drift(&h->base_max, &h->base_min); }
 
 // device error word: bit 0 overflow pool exhausted, bit 1 grid barrier wait gave up
 int device_fail(int e) {
@@ -246,8 +278,20 @@ void hpdmk_tree_destroy(hpdmk_tree tree) {
 int hpdmk_form_outgoing_pw(hpdmk_tree t) {
   if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
   return guarded([&]() {
-    DeviceGuard dg(H(t)->device);
-    H(t)->tree->form_outgoing_pw();
+    Handle* h = H(t);
+    DeviceGuard dg(h->device);
+    if (h->rebuild_factor > 1.0) {
+      int mx = 0, mn = 0;
+      h->tree->drift(&mx, &mn);
+      const double npl = double(h->tree->n_per_leaf());
+      if (mx > std::max(h->rebuild_factor * npl, double(h->base_max)) ||
+          mn < std::min(npl / h->rebuild_factor, double(h->base_min))) {
+        rebuild_structure(h);
+        ++h->rebuilds;
+        record_baseline(h);
+      }
+    }
+    h->tree->form_outgoing_pw();
     return ok();
   });
 }
@@ -561,25 +605,32 @@ int hpdmk_tree_rebuild(hpdmk_tree t) {
   Handle* h = H(t);
   return guarded([&]() {
     DeviceGuard dg(H(t)->device);
-    const pdmk::DmkTree& old = *h->tree;
-    const long n = old.n_particles();
-    double* d_r = nullptr;
-    PDMK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_r), sizeof(double) * 4 * size_t(n), h->stream));
-    double* d_q = d_r + 3 * n;
-    old.gather_device(d_r, d_q);
-    try {
-      auto nt = std::make_unique<pdmk::DmkTree>(old.box(), old.n_per_leaf(), old.digits(), n, d_r, d_q, true,
-                                                old.options(), h->stream);
-      nt->set_mc_mode(old.mc_mode());  // the caller's settings carry over
-      nt->set_tuning(old.tuning());
-      h->tree = std::move(nt);
-    } catch (...) {
-      cudaFreeAsync(d_r, h->stream);
-      throw;
-    }
-    PDMK_CUDA(cudaFreeAsync(d_r, h->stream));
+    rebuild_structure(h);
+    if (h->rebuild_factor > 1.0) record_baseline(h);
     h->tree->form_outgoing_pw();
     h->tree->form_incoming_pw();
+    return ok();
+  });
+}
+
+int hpdmk_set_rebuild_policy(hpdmk_tree t, double leaf_factor) {
+  if (!t) return fail(HPDMK_ERR_BAD_INPUT, "null tree");
+  if (!(leaf_factor == 0.0 || (leaf_factor > 1.0 && std::isfinite(leaf_factor))))
+    return fail(HPDMK_ERR_BAD_INPUT, "leaf_factor must be 0 (off) or a finite number above 1");
+  return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
+    H(t)->rebuild_factor = leaf_factor;
+    if (leaf_factor > 1.0) record_baseline(H(t));
+    return ok();
+  });
+}
+
+int hpdmk_tree_drift(hpdmk_tree t, int* max_leaf, int* min_refined, int* rebuilds) {
+  if (!t || !max_leaf || !min_refined) return fail(HPDMK_ERR_BAD_INPUT, "null argument");
+  return guarded([&]() {
+    DeviceGuard dg(H(t)->device);
+    H(t)->tree->drift(max_leaf, min_refined);
+    if (rebuilds) *rebuilds = H(t)->rebuilds;
     return ok();
   });
 }

@@ -248,6 +248,9 @@ class DmkTree {
   void export_positions(double* r_orig_order) const;
   // current positions [3n] and charges [n] in original order into device buffers (stream-ordered)
   void gather_device(double* d_r, double* d_q) const;
+  // the largest particle count of a leaf and the smallest of a refined node
+  // below level 2 (N when there is none), from the maintained node counts
+  void drift(int* max_leaf, int* min_refined) const;
   long n_particles() const { return N_; }
   int n_per_leaf() const { return n_per_leaf_; }
   int digits() const { return digits_; }

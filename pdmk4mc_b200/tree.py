@@ -140,6 +140,11 @@ def load_library():
     L.hpdmk_replicas_energy.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), _dp]
     L.hpdmk_tree_rebuild.restype = ctypes.c_int
     L.hpdmk_tree_rebuild.argtypes = [ctypes.c_void_p]
+    L.hpdmk_set_rebuild_policy.restype = ctypes.c_int
+    L.hpdmk_set_rebuild_policy.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    L.hpdmk_tree_drift.restype = ctypes.c_int
+    L.hpdmk_tree_drift.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_int)]
     L.hpdmk_ewald_energy.restype = ctypes.c_int
     L.hpdmk_ewald_energy.argtypes = [ctypes.c_void_p, _dp, _dp]
     L.hpdmk_set_mc_mode.restype = ctypes.c_int
@@ -283,6 +288,23 @@ class HPDMKPtTree:
 
     def form_outgoing_pw(self):
         _check(load_library().hpdmk_form_outgoing_pw(self._h))
+        if getattr(self, "_rebuild_factor", 0.0) > 0.0:
+            self._refresh_info()  # the rebuild policy may have re-binned the tree
+
+    def set_rebuild_policy(self, leaf_factor):
+        """With leaf_factor > 1, every form_outgoing_pw first rebuilds the tree
+        when a leaf holds more than leaf_factor * n_per_leaf particles or a
+        refined node below level 2 fewer than n_per_leaf / leaf_factor; 0 turns
+        the check off (hpdmk_set_rebuild_policy)."""
+        _check(load_library().hpdmk_set_rebuild_policy(self._h, float(leaf_factor)))
+        self._rebuild_factor = float(leaf_factor)
+
+    def drift(self):
+        """(largest leaf count, smallest refined-node count below level 2,
+        rebuilds made by the policy)."""
+        a, b, c = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        _check(load_library().hpdmk_tree_drift(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
 
     def form_incoming_pw(self):
         _check(load_library().hpdmk_form_incoming_pw(self._h))

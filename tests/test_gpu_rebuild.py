@@ -75,3 +75,51 @@ def test_rebuild_equals_fresh_tree(mode):
     finally:
         t.close()
         f.close()
+
+
+def test_rebuild_policy():
+    # particles pulled into one corner: leaves there overfill, so with the
+    # policy set the next full energy re-bins the tree first; its energy then
+    # equals a fresh tree of the moved positions, and without drift nothing
+    # is rebuilt
+    n, L, npl, digits = 3000, 12.0, 10, 6
+    rng = np.random.default_rng(41)
+    r = np.ascontiguousarray(rng.uniform(0, L, 3 * n))
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    params = P.HPDMKParams(n_per_leaf=npl, digits=digits, L=L, init=P.DIRECT)
+    t = P.HPDMKPtTree(params, r, q, leaf_slack=2, pool_capacity=8192)
+    try:
+        t.set_rebuild_policy(2.0)
+        t.form_outgoing_pw()
+        t.form_incoming_pw()
+        assert t.drift()[2] == 0
+        depth0 = t.max_depth
+        # move 600 particles towards the corner (1, 1, 1), all accepted (beta = 0)
+        idx = rng.choice(n, 600, replace=False)
+        pos = t.positions().reshape(-1, 3)
+        target = rng.uniform(0.5, 1.5, (600, 3))
+        disp = target - pos[idx]
+        _, acc = t.mc_run(idx, disp, np.zeros(600), 0.0)
+        assert acc.all()
+        mx, mn, nreb = t.drift()
+        assert mx > 2 * npl and nreb == 0
+        t.form_outgoing_pw()
+        t.form_incoming_pw()
+        E = t.eval_energy()
+        mx2, _, nreb = t.drift()
+        assert nreb == 1 and mx2 <= npl and t.max_depth > depth0
+        f = P.HPDMKPtTree(params, np.ascontiguousarray(t.positions()), q)
+        try:
+            f.form_outgoing_pw()
+            f.form_incoming_pw()
+            Ef = f.eval_energy()
+        finally:
+            f.close()
+        assert abs(E - Ef) <= REL_E * abs(Ef), (E, Ef)
+        # no drift since: no second rebuild
+        t.form_outgoing_pw()
+        assert t.drift()[2] == 1
+        with pytest.raises(P.HPDMKError):
+            t.set_rebuild_policy(0.5)
+    finally:
+        t.close()
