@@ -129,7 +129,8 @@ struct MixShape {
   static constexpr int STAGE_OUT = RPC * D * 16;  // epilogue staging, reuses the table stages
   static constexpr int SMEM = (PIPE_BYTES > STAGE_OUT ? PIPE_BYTES : STAGE_OUT) + 1024;  // + alignment slack
   // table kernel shared memory: coordinates, ex scratch, the block
-  static constexpr int TK_OFF_EX = (COORD_BYTES + 127) / 128 * 128;
+  static constexpr int TK_COORD_STRIDE = (COORD_BYTES + 127) / 128 * 128;  // two coordinate buffers
+  static constexpr int TK_OFF_EX = 2 * TK_COORD_STRIDE;
   static constexpr int TK_OFF_T = (TK_OFF_EX + KCP * D * 16 + 127) / 128 * 128;
   static constexpr int TK_SMEM = TK_OFF_T + T_STRIDE + 1024;
   static_assert(TCOLS_USED <= 512, "accumulators and A stages exceed TMEM");
@@ -271,95 +272,122 @@ __device__ void axis_factors_d(double xr, double dk, int M, int X, int m0, int c
 
 
 
-// Table pass: the FP64 phase factors of one chunk of one box, the sliced B
+// Table pass: the FP64 phase factors of a chunk of a box, the sliced B
 // operand in the tensor core's K-major layout and the ey, ez factors,
-// written to the chunk's table block. One thread per (particle, axis, half
-// of the mode range), consecutive lanes on consecutive particles.
+// written to the chunk's table block. Persistent: a CTA walks the chunks
+// blockIdx.x, blockIdx.x + gridDim.x, ...; the next chunk's coordinates come
+// in by TMA into the second coordinate buffer while the current chunk is
+// formed, and a block's bulk store to HBM runs on while the next chunk's
+// factors are formed (only its read of the block is awaited before the
+// block is reused). One thread per (particle, axis, half of the mode range),
+// consecutive lanes on consecutive particles.
 template <int NK>
 __global__ void __launch_bounds__(MixShape<NK>::TTHREADS)
     k_pw_tables(const __grid_constant__ CUtensorMap coords, const MixItem* __restrict__ items,
-                const int2* __restrict__ chunks, const double* __restrict__ qmax_p, int* __restrict__ err) {
+                const int2* __restrict__ chunks, int nchunks, const double* __restrict__ qmax_p,
+                int* __restrict__ err) {
   using S = MixShape<NK>;
   constexpr int D = S::D, NPAD = S::NPAD, HALF = S::HALF, KCP = S::KCP, KB = S::KB;
   extern __shared__ unsigned char smem_raw[];
   // the 1024-aligned base as an offset from the shared array, so that the
   // compiler keeps shared-memory (not generic) loads and stores
   unsigned char* sm = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar[2];
   const int tid = threadIdx.x;
-  const int2 ch = chunks[blockIdx.x];
-  const MixItem it = items[ch.x];
-  const int sb = it.s_begin + ch.y * KCP;
-  const int nk = min(KCP, it.s_end - sb);
-  const int off = sb - (sb & ~1);
   const double qmax = *qmax_p;
   const double inv_qmax = qmax > 0.0 ? 1.0 / qmax : 0.0;
-  const double* P = reinterpret_cast<const double*>(sm);
   double2* ex = reinterpret_cast<double2*>(sm + S::TK_OFF_EX);
   unsigned char* blk = sm + S::TK_OFF_T;
   double2* ey = reinterpret_cast<double2*>(blk + S::EY_OFF);
   double2* ez = reinterpret_cast<double2*>(blk + S::EZ_OFF);
+  auto chunk_start = [&](int q) {
+    const int2 c = chunks[q];
+    return items[c.x].s_begin + c.y * KCP;
+  };
+  auto load_coords = [&](int q, int b) {  // thread 0: chunk q's coordinates into buffer b
+    tc::mbar_arrive_expect_tx(&bar[b], S::COORD_BYTES);
+    tc::tma_load_2d(sm + b * S::TK_COORD_STRIDE, &coords, chunk_start(q) & ~1, 0, &bar[b]);
+  };
   if (tid == 0) {
-    tc::mbar_init(&bar, 1);
+    tc::mbar_init(&bar[0], 1);
+    tc::mbar_init(&bar[1], 1);
     tc::mbar_fence_init();
   }
   __syncthreads();
-  if (tid == 0) {
-    tc::mbar_arrive_expect_tx(&bar, S::COORD_BYTES);
-    tc::tma_load_2d(sm, &coords, sb & ~1, 0, &bar);
-  }
-  if (!tc::mbar_wait(&bar, 0)) atomicOr(err, 4);  // bounded; the zero-filled buffer is then still read safely
-  {
-    const int j = tid % KCP, ah = tid / KCP, a = ah >> 1, half = ah & 1;
-    const int len = a == 2 ? NK + 1 : D;
-    const int h0 = (len + 1) / 2;
-    const int m0 = half ? -NK + h0 : -NK, cnt = half ? len - h0 : h0;
-    double2* dst = (a == 0 ? ex + j * D : (a == 1 ? ey + j * D : ez + j * S::EZS)) + (m0 + NK);
-    if (j < nk) {
-      const double xa = P[a * S::COORD_BOX + off + j];
-      const double ca = a == 0 ? it.cx : (a == 1 ? it.cy : it.cz);
-      const int Xa = a == 0 ? it.X : (a == 1 ? it.Y : it.Z);
-      const double scale = a == 0 ? SL_SCALE : (a == 1 ? 1.0 : SL_SCALE * P[3 * S::COORD_BOX + off + j] * inv_qmax);
-      axis_factors_d(xa - ca, it.dk, it.M, Xa, m0, cnt, scale, dst);
-    } else {
-      for (int m = 0; m < cnt; ++m) dst[m] = make_double2(0.0, 0.0);
+  if (tid == 0 && int(blockIdx.x) < nchunks) load_coords(blockIdx.x, 0);
+  int i = 0;
+  for (int q = blockIdx.x; q < nchunks; q += gridDim.x, ++i) {
+    const int b = i & 1;
+    const int2 ch = chunks[q];
+    const MixItem it = items[ch.x];
+    const int sb = it.s_begin + ch.y * KCP;
+    const int nk = min(KCP, it.s_end - sb);
+    const int off = sb - (sb & ~1);
+    const double* P = reinterpret_cast<const double*>(sm + b * S::TK_COORD_STRIDE);
+    if (tid == 0) {
+      // the other buffer's last reader finished before the previous
+      // iteration's last barrier
+      if (q + int(gridDim.x) < nchunks) load_coords(q + gridDim.x, b ^ 1);
+      // the previous chunk's store has read the block
+      tc::bulk_wait_read_all();
     }
-  }
-  __syncthreads();
-  // B operand from ex: column n < D of each slice is the real part of mode
-  // kx = n, column HALF + kx its imaginary part; K rows (2j, 2j+1) carry
-  // (Br, -Bi) for a real column and (Bi, Br) for an imaginary one
-  const uint32_t bbase = tc::smem_u32(blk);
-  for (int task = tid; task < NPAD * (KB / 16); task += S::TTHREADS) {
-    const int n = task % NPAD, kc = task / NPAD;
-    uint32_t w[4][4];
-    const bool re = n < D, im = n >= HALF && n < HALF + D;
-    const int kx = re ? n : n - HALF;
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      const int j0 = kc * 8 + 2 * p;
-      double2 v0 = make_double2(0.0, 0.0), v1 = make_double2(0.0, 0.0);
-      if (re || im) {
-        const double2 e0 = ex[j0 * D + kx], e1 = ex[(j0 + 1) * D + kx];
-        v0 = re ? make_double2(e0.x, -e0.y) : make_double2(e0.y, e0.x);
-        v1 = re ? make_double2(e1.x, -e1.y) : make_double2(e1.y, e1.x);
+    // bounded; the zero-filled buffer is then still read safely
+    if (!tc::mbar_wait(&bar[b], uint32_t(i >> 1) & 1)) atomicOr(err, 4);
+    __syncthreads();
+    {
+      const int j = tid % KCP, ah = tid / KCP, a = ah >> 1, half = ah & 1;
+      const int len = a == 2 ? NK + 1 : D;
+      const int h0 = (len + 1) / 2;
+      const int m0 = half ? -NK + h0 : -NK, cnt = half ? len - h0 : h0;
+      double2* dst = (a == 0 ? ex + j * D : (a == 1 ? ey + j * D : ez + j * S::EZS)) + (m0 + NK);
+      if (j < nk) {
+        const double xa = P[a * S::COORD_BOX + off + j];
+        const double ca = a == 0 ? it.cx : (a == 1 ? it.cy : it.cz);
+        const int Xa = a == 0 ? it.X : (a == 1 ? it.Y : it.Z);
+        const double scale =
+            a == 0 ? SL_SCALE : (a == 1 ? 1.0 : SL_SCALE * P[3 * S::COORD_BOX + off + j] * inv_qmax);
+        axis_factors_d(xa - ca, it.dk, it.M, Xa, m0, cnt, scale, dst);
+      } else {
+        for (int m = 0; m < cnt; ++m) dst[m] = make_double2(0.0, 0.0);
       }
-      uint32_t by[4];
-      transpose4(fix24(v0.x), fix24(v0.y), fix24(v1.x), fix24(v1.y), by);
-#pragma unroll
-      for (int sl = 0; sl < 4; ++sl) w[sl][p] = by[3 - sl];  // slice 0 = the top byte
     }
+    __syncthreads();
+    // B operand from ex: column n < D of each slice is the real part of mode
+    // kx = n, column HALF + kx its imaginary part; K rows (2j, 2j+1) carry
+    // (Br, -Bi) for a real column and (Bi, Br) for an imaginary one
+    const uint32_t bbase = tc::smem_u32(blk);
+    for (int task = tid; task < NPAD * (KB / 16); task += S::TTHREADS) {
+      const int n = task % NPAD, kc = task / NPAD;
+      uint32_t w[4][4];
+      const bool re = n < D, im = n >= HALF && n < HALF + D;
+      const int kx = re ? n : n - HALF;
 #pragma unroll
-    for (int sl = 0; sl < 4; ++sl)
-      st_shared_v4(bbase + kc * S::B_KGROUP + (sl * NPAD + n) * 16, w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
+      for (int p = 0; p < 4; ++p) {
+        const int j0 = kc * 8 + 2 * p;
+        double2 v0 = make_double2(0.0, 0.0), v1 = make_double2(0.0, 0.0);
+        if (re || im) {
+          const double2 e0 = ex[j0 * D + kx], e1 = ex[(j0 + 1) * D + kx];
+          v0 = re ? make_double2(e0.x, -e0.y) : make_double2(e0.y, e0.x);
+          v1 = re ? make_double2(e1.x, -e1.y) : make_double2(e1.y, e1.x);
+        }
+        uint32_t by[4];
+        transpose4(fix24(v0.x), fix24(v0.y), fix24(v1.x), fix24(v1.y), by);
+#pragma unroll
+        for (int sl = 0; sl < 4; ++sl) w[sl][p] = by[3 - sl];  // slice 0 = the top byte
+      }
+#pragma unroll
+      for (int sl = 0; sl < 4; ++sl)
+        st_shared_v4(bbase + kc * S::B_KGROUP + (sl * NPAD + n) * 16, w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
+    }
+    tc::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::bulk_store(const_cast<unsigned char*>(it.tab) + size_t(ch.y) * S::T_BYTES, blk, S::T_BYTES);
+      tc::bulk_commit();
+    }
   }
-  tc::fence_async_smem();
-  __syncthreads();
-  if (tid == 0) {
-    tc::bulk_store(const_cast<unsigned char*>(it.tab) + size_t(ch.y) * S::T_BYTES, blk, S::T_BYTES);
-    tc::bulk_commit();
-    tc::bulk_wait_all();
-  }
+  // the stores complete before the CTA ends
+  if (tid == 0) tc::bulk_wait_all();
 }
 
 // Contraction: one 128-row M tile of one box (or split-K chunk) over its
@@ -580,7 +608,15 @@ void launch_mixed(const CUtensorMap& tmap, const MixItem* d_items, int nitems, c
   if (nitems == 0) return;
   if (nchunks > 0) {
     raise_smem_limit(reinterpret_cast<const void*>(k_pw_tables<NK>), S::TK_SMEM);
-    k_pw_tables<NK><<<unsigned(nchunks), S::TTHREADS, S::TK_SMEM, st>>>(tmap, d_items, d_chunks, d_qmax, d_err);
+    // persistent: as many CTAs as are resident at once, each walking a
+    // strided share of the chunks
+    int dev = 0, sms = 0, per_sm = 0;
+    PDMK_CUDA(cudaGetDevice(&dev));
+    PDMK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    PDMK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pw_tables<NK>, S::TTHREADS, S::TK_SMEM));
+    const int grid = std::max(1, std::min(nchunks, std::max(1, per_sm) * sms));
+    k_pw_tables<NK><<<unsigned(grid), S::TTHREADS, S::TK_SMEM, st>>>(tmap, d_items, d_chunks, nchunks, d_qmax,
+                                                                       d_err);
     PDMK_LAUNCH_CHECK();
   }
   raise_smem_limit(reinterpret_cast<const void*>(k_pw_mixed<NK>), S::SMEM);
