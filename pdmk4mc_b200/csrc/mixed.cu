@@ -93,10 +93,16 @@ template <int NK>
 struct MixShape {
   static constexpr int D = 2 * NK + 1;
   static constexpr int ROWS = (NK + 1) * D;  // row r = kz D + ky, as the expansion's layout
+  // rows computed: the kz < 0 planes whole, the kz = 0 plane for ky >= 0
+  // only; its ky < 0 rows follow by conjugate symmetry (real charges:
+  // out(-k) = conj(out(k))). Computed row rho maps to r = rho below NK D and
+  // to r = rho + NK above.
+  static constexpr int ROWS_C = NK * D + NK + 1;
+  static_assert(ROWS_C <= ROWS, "computed rows");
   static constexpr int NPAD = npad_of(NK);  // MMA N: Re columns [0, D), Im columns [HALF, HALF + D)
   static constexpr int HALF = NPAD / 2;
   static constexpr int EZS = ezs_of(NK);    // odd row strides keep 16-byte stores on distinct bank groups
-  static constexpr int TILES = (ROWS + RPC - 1) / RPC;  // CTAs per box
+  static constexpr int TILES = (ROWS_C + RPC - 1) / RPC;  // CTAs per box
   static constexpr int KCP = chunk32_fits(NK) ? 32 : 16;  // particles per chunk
   static constexpr int KB = 2 * KCP;        // K bytes per chunk (real and imaginary part per particle)
   static constexpr int KSTEPS = KB / 32;    // MMA K steps (32 bytes each) per chunk
@@ -410,8 +416,8 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
   const int warp = tid >> 5;
   const bool control = tid >= S::CTHREADS;
   const MixItem it = items[blockIdx.x];
-  const int row0 = it.pair * RPC;
-  const int nrows = min(RPC, S::ROWS - row0);  // valid rows of this CTA
+  const int row0 = it.pair * RPC;                 // first computed row of this CTA
+  const int nrows = min(RPC, S::ROWS_C - row0);  // valid rows of this CTA
   const int nch = (it.s_end - it.s_begin + KCP - 1) / KCP;
   const double qmax = *qmax_p;
 
@@ -495,8 +501,9 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
     // ------------------------------------------------------------ consumers
     const int lr = tid & (RPC - 1);  // local row = TMEM lane
     const int kh = tid / RPC;        // this thread's 16-byte K group (8 particles) of each chunk
-    const int r = row0 + lr;
+    const int rho = row0 + lr;
     const bool active = lr < nrows;
+    const int r = rho < NK * D ? rho : rho + NK;  // the expansion row
     const int kz = active ? r / D : 0, ky = active ? r % D : 0;
     // this thread's four A columns of slice 0 of stage 0 (its warp's lane quarter)
     const uint32_t arow = tmem + (uint32_t(32 * (warp & 3)) << 16) + uint32_t(S::A_COL0 + kh * 4);
@@ -565,11 +572,28 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
     }
     tc::fence_async_smem();
     tc::bar_sync(BAR_CONS, S::CTHREADS);
+    // computed rows below NK D are the expansion rows themselves; those above
+    // lie NK rows further on (the kz = 0, ky >= 0 rows)
+    const int n_lo = max(0, min(nrows, NK * D - row0));
     if (tid == 0) {
-      tc::bulk_store(it.out + size_t(row0) * D, sm, uint32_t(nrows) * D * 16u);
+      if (n_lo > 0) tc::bulk_store(it.out + size_t(row0) * D, sm, uint32_t(n_lo) * D * 16u);
+      if (nrows > n_lo)
+        tc::bulk_store(it.out + size_t(row0 + n_lo + NK) * D, sm + size_t(n_lo) * D * 16, uint32_t(nrows - n_lo) * D * 16u);
       tc::bulk_commit();
-      tc::bulk_wait_all();
     }
+    // the kz = 0, ky < 0 rows: out[NK][ky][kx] = conj(out[NK][2 NK - ky][2 NK - kx])
+    // from the staged rows ky = 2 NK - ky > NK of this CTA
+    {
+      const double2* st0 = reinterpret_cast<const double2*>(sm);
+      const int m_lo = max(row0, NK * D + 1), m_hi = row0 + nrows;  // computed rows with ky > NK
+      for (int idx = tid; idx < (m_hi - m_lo) * D; idx += S::CTHREADS) {
+        const int src = m_lo + idx / D, kx = idx % D;
+        const int ky = NK + (src - NK * D);          // > NK
+        const double2 v = st0[size_t(src - row0) * D + (2 * NK - kx)];
+        it.out[size_t(NK * D + 2 * NK - ky) * D + kx] = make_double2(v.x, -v.y);
+      }
+    }
+    if (tid == 0) tc::bulk_wait_all();
   }
   // copies and MMAs this CTA started have ended (bounded waits; they only
   // matter when a pipeline wait gave up) before its TMEM is released
