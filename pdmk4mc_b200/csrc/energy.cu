@@ -892,10 +892,12 @@ int DmkTree::res_chunks() const {
 
 void DmkTree::set_tuning(const Tuning& t) {
   Tuning c = t;
-  // the mixed pass's exact int32 sums hold at most 16384 particles per
-  // split-K chunk (four signed 8-bit slice products of up to 2^14 per
-  // accumulator and K entry, two K entries per particle); half of it is allowed
-  const int cap = opt_.precision == 1 ? 8192 : 1 << 20;
+  // the mixed pass's exact int32 sums hold 16384 particles per split-K
+  // chunk: an accumulator takes at most four slice products per K entry, top
+  // digits lie in [-127, 127] and lower ones in [-128, 127], so one K entry
+  // adds at most 2 127 128 + 2 128^2 = 65280, and two K entries per particle
+  // give 2 16384 65280 < 2^31
+  const int cap = opt_.precision == 1 ? 16384 : 1 << 20;
   c.ksplit = std::min(cap, std::max(256, c.ksplit));
   c.ksplit_root = std::min(cap, std::max(256, c.ksplit_root));
   c.inc_waves = std::min(64, std::max(1, c.inc_waves));

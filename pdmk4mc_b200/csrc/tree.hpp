@@ -365,7 +365,7 @@ class DmkTree {
   int precision() const { return opt_.precision; }
   const Tuning& tuning() const { return tune_; }
   // clamps to the supported ranges (the mixed pass's exact int32 sums bound
-  // a split-K chunk to 8192 particles)
+  // a split-K chunk to 16384 particles)
   void set_tuning(const Tuning& t);
   // times one phase of the energy pipeline (0 outgoing, 1 incoming, 2 near
   // field) `reps` times on the tree's stream; returns the median milliseconds

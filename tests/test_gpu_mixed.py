@@ -164,3 +164,38 @@ def test_mixed_bench_workload_vs_ewald():
     finally:
         g.close()
         f.close()
+
+
+def test_mixed_largest_split_k_chunk():
+    # one level-2 box holds 20 000 particles, so with ksplit = 16384 one
+    # split-K chunk carries the most particles the exact int32 sums allow;
+    # expansions and energy against the FP64 path (parity-tested against the
+    # oracle elsewhere)
+    rng = np.random.default_rng(9)
+    L, n_in, n_out = 24.0, 20000, 4000
+    r = np.concatenate([rng.uniform(0.5, 5.5, (n_in, 3)), rng.uniform(0, L, (n_out, 3))])
+    r = np.ascontiguousarray(r.reshape(-1))
+    n = n_in + n_out
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    prm = P.HPDMKParams(n_per_leaf=400, digits=9, L=L, init=P.DIRECT)
+    g = P.HPDMKPtTree(prm, r, q, precision=P.PRECISION_MIXED)
+    f = P.HPDMKPtTree(prm, r, q)
+    try:
+        g.set_tuning(ksplit=16384, ksplit_root=16384)
+        assert g.tuning()["ksplit"] == 16384
+        for t in (g, f):
+            t.form_outgoing_pw()
+            t.form_incoming_pw()
+        rg, rf = g.pw(0), f.pw(0)
+        assert np.abs(rg - rf).max() <= REL_PW_MIXED * np.abs(rf).max()
+        lv, pf, leaf, cnt = O.OracleTree(L, 400, 9, r, q).tree_nodes()
+        big = [int(b) for b in np.nonzero((lv == 2) & (cnt > 16384))[0]]
+        assert big, "no box above the chunk size"
+        for b in big:
+            a, c = g.pw(b), f.pw(b)
+            assert np.abs(a - c).max() <= REL_PW_MIXED * np.abs(c).max()
+        Em, Ef = g.eval_energy(), f.eval_energy()
+        assert abs(Em - Ef) <= rel_e_mixed(9) * abs(Ef), (Em, Ef)
+    finally:
+        g.close()
+        f.close()

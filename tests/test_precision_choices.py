@@ -72,10 +72,13 @@ def test_int8_slice_contraction_of_one_box():
     scale = qmax / (127.0 * 127.0)
     w = [256.0 ** -k for k in range(4)]
     out = scale * (sum(a * c for a, c in zip(acc_re, w)) + 1j * sum(a * c for a, c in zip(acc_im, w)))
-    # the digits are signed bytes, and the exact integer sums fit 32 bits for
-    # a split-K chunk of 8192 particles
+    # the digits are signed bytes with top digits in [-127, 127], so the exact
+    # integer sums fit 32 bits for a split-K chunk of 16384 particles: at most
+    # four products per accumulator and K entry, two K entries per particle
     assert all(np.abs(a).max() <= 128 for a in sa_r + sa_i + sb_r + sb_i)
-    assert max(np.abs(a).max() for a in acc_re + acc_im) * 8192 / n_box < 2 ** 31
+    assert all(np.abs(a[0]).max() <= 127 for a in (sa_r, sa_i, sb_r, sb_i))
+    assert 2 * 16384 * (2 * 127 * 128 + 2 * 128 * 128) < 2 ** 31
+    assert max(np.abs(a).max() for a in acc_re + acc_im) * 16384 / n_box < 2 ** 31
     err = np.abs(out - ref).max() / np.abs(ref).max()
     rms = np.sqrt(np.mean(np.abs(out - ref) ** 2)) / np.sqrt(n_box)
     print(f"\nint8 slices, one box of {n_box}: max error {err:.2e} of the largest coefficient, "
