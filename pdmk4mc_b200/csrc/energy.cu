@@ -619,13 +619,20 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
   __shared__ int m_beg[36], m_pre[37];
   __shared__ double m_off[36][3], m_w[36];
   __shared__ double sm[32];
+  // per warp, the pairs inside the cut-off waiting for a polynomial: r^2 and
+  // q_target q_source (at most 31 waiting plus 32 added in one step)
+  __shared__ double q_r2[RES_T / 32][64], q_w[RES_T / 32][64];
   const ResidualPoly<NP> poly(T);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int qn = 0;  // pairs waiting in this warp's queue (warp-uniform)
   const int node = leaves[blockIdx.x / ny], chunk = blockIdx.x % ny;
   const int l = T.node_level[node];
   const int cnt = T.leaf_count[node];
   double e = 0;
+  double inv_b_all = 0;
   if (l >= 2 && cnt > chunk * RES_TCH) {
     const double b = level_box(T, l), inv_b = 1.0 / b;
+    inv_b_all = inv_b;
     const double b2 = b * b * (1.0 + 1e-14);  // square roots only near or inside the cut-off
     const int tb = T.node_begin[node];
     if (threadIdx.x < 36) {
@@ -684,7 +691,6 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
         tz = T.sz[tslot];
         tq = T.sq[tslot];
       }
-      double et = 0;
       for (int u0 = 0; u0 < total; u0 += RES_SCH) {
         const int ns = min(RES_SCH, total - u0);
         __syncthreads();
@@ -704,32 +710,46 @@ __global__ void __launch_bounds__(RES_T) k_residual(DevTree T, const int* __rest
           uslot[t] = lo == 0 ? s : -1;
         }
         __syncthreads();
-        // two sources per step: their Horner chains are independent, so each
-        // hides the other's FMA latency
-        if (act)
-          for (int js = sp; js < ns; js += 2 * nparts) {
-            const int j2 = js + nparts;
-            const double dxa = tx - ux[js], dya = ty - uy[js], dza = tz - uz[js];
-            const double r2a = dxa * dxa + dya * dya + dza * dza;
-            const bool ina = r2a <= b2 && uslot[js] != tslot;
-            bool inb = false;
-            double r2b = 0;
-            if (j2 < ns) {
-              const double dxb = tx - ux[j2], dyb = ty - uy[j2], dzb = tz - uz[j2];
-              r2b = dxb * dxb + dyb * dyb + dzb * dzb;
-              inb = r2b <= b2 && uslot[j2] != tslot;
-            }
-            if (ina || inb) {
-              // from_r2 is zero at and beyond the cut-off
-              const double pa = poly.from_r2(ina ? r2a : 0.0, inv_b), pb = poly.from_r2(inb ? r2b : 0.0, inv_b);
-              et += uq[js] * pa;
-              if (j2 < ns) et += uq[j2] * pb;
-            }
+        // About one pair in six lies inside the cut-off, and a warp would run
+        // the Horner chain whenever any lane needs it: the lanes push their
+        // in-range pairs into the warp's queue instead, and the warp
+        // evaluates the polynomial 32 queued pairs at a time. The loop is
+        // warp-uniform (every lane of a warp has the same source partition).
+        for (int js = sp; js < ns; js += nparts) {
+          const double dx = tx - ux[js], dy = ty - uy[js], dz = tz - uz[js];
+          const double r2 = dx * dx + dy * dy + dz * dz;
+          const bool in = act && r2 <= b2 && uslot[js] != tslot;
+          const unsigned m = __ballot_sync(0xffffffffu, in);
+          if (in) {
+            const int pos = qn + __popc(m & ((1u << lane) - 1u));
+            q_r2[wid][pos] = r2;
+            q_w[wid][pos] = tq * uq[js];
           }
+          qn += __popc(m);
+          if (qn >= 32) {
+            __syncwarp();
+            e += q_w[wid][lane] * poly.from_r2(q_r2[wid][lane], inv_b);  // from_r2 is zero beyond the cut-off
+            const int rem = qn - 32;
+            double r2m = 0, wm = 0;
+            if (lane < rem) {
+              r2m = q_r2[wid][32 + lane];
+              wm = q_w[wid][32 + lane];
+            }
+            __syncwarp();
+            if (lane < rem) {
+              q_r2[wid][lane] = r2m;
+              q_w[wid][lane] = wm;
+            }
+            __syncwarp();
+            qn = rem;
+          }
+        }
       }
-      e += tq * et;
     }
   }
+  // the pairs still queued
+  __syncwarp();
+  if (lane < qn) e += q_w[wid][lane] * poly.from_r2(q_r2[wid][lane], inv_b_all);
   double s = block_sum(0.5 * e, sm);
   if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
