@@ -149,19 +149,21 @@ int hpdmk_eval_shift_energy_batch(hpdmk_tree tree, int m, const long *i, const d
  * without a host synchronisation (one launch, one thread block per candidate). */
 int hpdmk_eval_shift_energy_batch_device(hpdmk_tree tree, int m, const int *d_i, const double *d_d, double *d_dE);
 
-/* No reference counterpart. Same results as hpdmk_eval_shift_energy_batch, but
- * the call allocates no device memory: its block partials, completion counter,
- * proposal record, phase tables and staged inputs/outputs live in one fixed
- * static device buffer (about 250 KB per device, found once per device). For
- * callers that may not allocate device memory once the tree exists: a process
- * that budgets its device memory up front, or one whose memory is handed out
- * by another framework's pool that it must not grow or bypass.
+/* No reference counterpart. The same single launch as
+ * hpdmk_eval_shift_energy_batch (one thread block per candidate, phase tables
+ * in shared memory), so the same results bit for bit, but the call allocates
+ * no device memory: the candidates' indices and displacements and their
+ * energy shifts are staged through one fixed static device array (144 KB per
+ * device, its address looked up once per device). For callers that may not
+ * allocate device memory once the tree exists: a process that budgets its
+ * device memory up front, or one whose memory is handed out by another
+ * framework's pool that it must not grow or bypass.
  * Limits: m <= HPDMK_STATIC_MAX_MOVES; larger m returns HPDMK_ERR_BAD_INPUT
- * with a message and does no work. The buffer keeps the last call's contents;
- * its completion counter must start at zero, and each call clears it.
- * Calls that overlap in time on one device share the buffer and race: make
- * them one after another. Make the first call on each device before any
- * stream capture starts, since it looks up the buffer's address. */
+ * with a message and does no work. Nothing in the array has to start at zero
+ * (each call writes the inputs it reads). Calls that overlap in time on one
+ * device share the array and race: make them one after another. Make the
+ * first call on each device before any stream capture starts, since it looks
+ * up the array's address. */
 #define HPDMK_STATIC_MAX_MOVES 4096
 int hpdmk_eval_shift_energy_batch_static(hpdmk_tree tree, int m, const long *i, const double *d, double *dE);
 
