@@ -12,8 +12,11 @@
 // is one real matrix product over K = 2 x (particles):
 //   [Re | Im](rows x 2d) = [Ar Ai](rows x 2K) . [[Br, Bi], [-Bi, Br]](2K x 2d).
 // Both operands lie in [-1, 1] after the scaling below. Each value v is formed
-// in FP64 and written in 32-bit fixed point, X = round(127 v 2^24), with one
-// FMA (adding 1.5 * 2^52 rounds to an integer that lands in the low word),
+// in FP64 and written in 32-bit fixed point, X = round(127 v 2^24) (adding
+// 1.5 * 2^52 rounds to an integer that lands in the low word): one FMA for
+// B; for A the product's two terms are added into that constant by two
+// FMAs, each rounding to an integer (ez carries the factor 2^24), so X is
+// within one unit instead of half a unit. X is written
 // as four signed base-256 digits, X = a1 2^24 + a2 2^16 + a3 2^8 + a4 with
 // every a_s in [-128, 127]: the bytes of Y = X + 0x808080 (folded into the
 // FMA's constant) with the top bit of the three lower bytes flipped. Signed
@@ -25,7 +28,8 @@
 // exact, so the sum over a box's particles adds no rounding at all; the
 // accumulators are combined in FP64 at the end,
 //   out = qmax / 127^2 (acc_2 + acc_3 / 2^8 + acc_4 / 2^16 + acc_5 / 2^24).
-// The operand error is the rounding of X (2.3e-10 of the operand's range) and
+// The operand error is the rounding of X (2.3e-10 of the operand's range for
+// B, twice that at most for A) and
 // the dropped products (s + t > 5, below 1e-9 of the range). This is the slice
 // splitting of Ozaki, Ogita and Oishi (error-free splitting of
 // floating-point products) in the fixed-point form of Ootomo, Ozaki and
@@ -158,6 +162,14 @@ constexpr double SL_SCALE = 127.0;  // operands are scaled to |t| <= 127
 // (y_i - 128) 256^i, and y_i - 128 is byte y_i with its top bit flipped.
 __device__ __forceinline__ uint32_t fix24(double t) {
   return uint32_t(__double2loint(fma(t, 16777216.0, 6755399449477248.0))) ^ 0x808080u;
+}
+
+// The digits word of X = round(a b + round(c d)) for |a b + c d| 2^-24 <= 127
+// with a, b, c, d already carrying the factor 2^24: two FMAs into the
+// rounding constant of fix24 (each rounds to an integer, so X is within one
+// unit of (a b + c d) instead of half a unit)
+__device__ __forceinline__ uint32_t fix24_dot(double a, double b, double c, double d) {
+  return uint32_t(__double2loint(fma(a, b, fma(c, d, 6755399449477248.0)))) ^ 0x808080u;
 }
 
 // bytes of four words transposed: out[b] = [w0.byte b, w1.byte b, w2.byte b, w3.byte b]
@@ -351,7 +363,7 @@ __global__ void __launch_bounds__(MixShape<NK>::TTHREADS)
         const double ca = a == 0 ? it.cx : (a == 1 ? it.cy : it.cz);
         const int Xa = a == 0 ? it.X : (a == 1 ? it.Y : it.Z);
         const double scale =
-            a == 0 ? SL_SCALE : (a == 1 ? 1.0 : SL_SCALE * P[3 * S::COORD_BOX + off + j] * inv_qmax);
+            a == 0 ? SL_SCALE : (a == 1 ? 1.0 : SL_SCALE * 16777216.0 * P[3 * S::COORD_BOX + off + j] * inv_qmax);
         axis_factors_d(xa - ca, it.dk, it.M, Xa, m0, cnt, scale, dst);
       } else {
         for (int m = 0; m < cnt; ++m) dst[m] = make_double2(0.0, 0.0);
@@ -522,10 +534,13 @@ __global__ void __launch_bounds__(MixShape<NK>::THREADS, 1)
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
           const int j0 = kh * 8 + 2 * p;
-          const double2 v0 = cmul_d(ez[j0 * S::EZS + kz], ey[j0 * D + ky]);
-          const double2 v1 = cmul_d(ez[(j0 + 1) * S::EZS + kz], ey[(j0 + 1) * D + ky]);
+          // A = ez ey with ez carrying 2^24: each component in fixed point
+          // from two FMAs
+          const double2 z0 = ez[j0 * S::EZS + kz], y0 = ey[j0 * D + ky];
+          const double2 z1 = ez[(j0 + 1) * S::EZS + kz], y1 = ey[(j0 + 1) * D + ky];
           uint32_t by[4];
-          transpose4(fix24(v0.x), fix24(v0.y), fix24(v1.x), fix24(v1.y), by);
+          transpose4(fix24_dot(z0.x, y0.x, -z0.y, y0.y), fix24_dot(z0.x, y0.y, z0.y, y0.x),
+                     fix24_dot(z1.x, y1.x, -z1.y, y1.y), fix24_dot(z1.x, y1.y, z1.y, y1.x), by);
 #pragma unroll
           for (int sl = 0; sl < 4; ++sl) w[sl][p] = by[3 - sl];
         }
