@@ -199,3 +199,66 @@ def test_mixed_largest_split_k_chunk():
     finally:
         g.close()
         f.close()
+
+
+def test_mixed_edge_cases():
+    """The mixed path at the edges the FP64 parity test covers: a single
+    charge (its periodic self-image energy, against the oracle), boundary
+    coordinates and a multi-box wrap (against the FP64 tree and the oracle),
+    and a system of zero charges, whose fixed-point scale max|q| is zero (every
+    expansion, energy and shift exactly zero)."""
+    L = 8.0
+    r1, q1 = np.array([1.0, 2.0, 3.0]), np.array([1.0])
+    g = P.HPDMKPtTree(P.HPDMKParams(n_per_leaf=4, digits=9, L=L, init=P.DIRECT), r1, q1,
+                      precision=P.PRECISION_MIXED)
+    o = O.OracleTree(L, 4, 9, r1, q1)
+    try:
+        for t in (g, o):
+            t.form_outgoing_pw()
+            t.form_incoming_pw()
+        Eg, Eo = g.eval_energy(), o.eval_energy()
+        assert abs(Eg - Eo) <= rel_e_mixed(9) * max(1.0, abs(Eo)), (Eg, Eo)
+        assert abs(g.eval_shift_energy(0, 1.5, -2.0, 7.9)) <= ABS_DE_MIXED
+    finally:
+        g.close()
+
+    rng = np.random.default_rng(4)
+    r = rng.uniform(0, L, (500, 3))
+    r[0] = [0.0, 0.0, 0.0]
+    r[1] = [np.nextafter(L, 0), np.nextafter(L, 0), 0.0]
+    r[2] = [L / 2, L / 4, L / 8]
+    r = np.ascontiguousarray(r.reshape(-1))
+    q = np.where(np.arange(500) % 2 == 0, 1.0, -1.0)
+    params = P.HPDMKParams(n_per_leaf=6, digits=9, L=L, init=P.DIRECT)
+    g = P.HPDMKPtTree(params, r, q, precision=P.PRECISION_MIXED)
+    f = P.HPDMKPtTree(params, r, q, precision=P.PRECISION_FP64)
+    o = O.OracleTree(L, 6, 9, r, q)
+    try:
+        for t in (g, f, o):
+            t.form_outgoing_pw()
+            t.form_incoming_pw()
+        Eo = o.eval_energy()
+        assert abs(g.eval_energy() - Eo) <= rel_e_mixed(9) * abs(Eo), (g.eval_energy(), Eo)
+        for i, d in [(0, (L, 0.0, 0.0)), (1, (1e-9, 0.0, -1e-9)), (2, (0.0, 0.0, 0.0)),
+                     (3, (-2.5 * L, 3.25 * L, 0.5))]:
+            dg, df, do = g.eval_shift_energy(i, *d), f.eval_shift_energy(i, *d), o.eval_shift_energy(i, *d)
+            assert abs(dg - df) <= ABS_DE_MIXED * max(1.0, abs(df)), (i, d, dg, df)
+            assert abs(dg - do) <= ABS_DE_MIXED * max(1.0, abs(do)), (i, d, dg, do)
+            for t in (g, f, o):
+                t.update_shift(i, *d)
+        np.testing.assert_array_equal(g.positions(), o.positions())
+        Eg, Ef = g.eval_energy(), f.eval_energy()
+        assert abs(Eg - Ef) <= rel_e_mixed(9) * abs(Ef), (Eg, Ef)
+    finally:
+        g.close()
+        f.close()
+
+    q0 = np.zeros(500)
+    g = P.HPDMKPtTree(params, r, q0, precision=P.PRECISION_MIXED)
+    try:
+        g.form_outgoing_pw()
+        g.form_incoming_pw()
+        assert g.eval_energy() == 0.0
+        assert g.eval_shift_energy(7, 0.3, -0.2, 0.1) == 0.0
+    finally:
+        g.close()
