@@ -3,7 +3,9 @@ numpy on the same inputs the kernels see.
 
 1. The outgoing expansion of one box from 8-bit slices: the kernel's
    arithmetic (FP64 phase factors, the 32-bit fixed point X = round(127 v
-   2^24) written as four signed base-256 digits, the ten slice products of
+   2^24) (for A each component rounded in two steps, as the kernel's two
+   FMAs do: the second term to an integer, then the sum) written as four
+   signed base-256 digits, the ten slice products of
    order s + t <= 5 summed exactly in integers, FP64 combination) against the FP64
    direct NUDFT of the reference (include/nudft.hpp:95-121). The
    coefficient error stays near 1e-9 of the largest coefficient.
@@ -32,13 +34,29 @@ def f32(x):
     return np.asarray(x, dtype=np.float32)
 
 
-def slices(t):
-    """t (|t| <= 127) -> the signed base-256 digits of X = round(t 2^24),
-    highest first, t ~ sum_s a_s 256^-s, every a_s in [-128, 127]: the bytes
-    of X + 0x808080, the three lower ones less 128."""
-    Y = np.rint(t * 2.0 ** 24).astype(np.int64) + 0x808080
+def digits(X):
+    """X (a 32-bit fixed point, |X| <= 127 2^24) -> its signed base-256
+    digits, highest first, X = sum_s a_s 256^(3-s), every a_s in [-128, 127]:
+    the bytes of X + 0x808080, the three lower ones less 128."""
+    Y = np.asarray(X).astype(np.int64) + 0x808080
     top = Y >> 24  # arithmetic shift: the signed top digit
     return [top, ((Y >> 16) & 0xFF) - 128, ((Y >> 8) & 0xFF) - 128, (Y & 0xFF) - 128]
+
+
+def slices(t):
+    """t (|t| <= 127) -> the digits of X = round(t 2^24)."""
+    return digits(np.rint(t * 2.0 ** 24))
+
+
+def slices_two_step(z, y):
+    """The digits of A = z y's components as the kernel forms them, z already
+    carrying 2^24: Re = round(round(-z.im y.im) + z.re y.re) and Im =
+    round(round(z.im y.re) + z.re y.im) (each FMA rounds to an integer; the
+    products here are rounded to FP64 first, which differs from the fused
+    product only within 2^-22 of a half-integer)."""
+    re = np.rint(np.rint(-z.imag * y.imag) + z.real * y.real)
+    im = np.rint(np.rint(z.imag * y.real) + z.real * y.imag)
+    return digits(re), digits(im)
 
 
 def test_int8_slice_contraction_of_one_box():
@@ -57,9 +75,10 @@ def test_int8_slice_contraction_of_one_box():
     ref = np.einsum("jz,jy,jx->zyx", ez, ey, ex)
     # the kernel: FP64 factors (ex scaled by 127, ez by 127 q / max|q|), A = ez ey in FP64
     qmax = np.abs(q).max()
-    A = (127 * ez / qmax)[:, :, None] * ey[:, None, :]  # [j, kz, ky]
+    z = (127 * 2.0 ** 24 * ez / qmax)[:, :, None]  # [j, kz, 1]
     B = 127 * ex
-    sa_r, sa_i, sb_r, sb_i = slices(A.real), slices(A.imag), slices(B.real), slices(B.imag)
+    sa_r, sa_i = slices_two_step(z, ey[:, None, :])  # [j, kz, ky]
+    sb_r, sb_i = slices(B.real), slices(B.imag)
     acc_re = [0, 0, 0, 0]
     acc_im = [0, 0, 0, 0]
     for s in range(4):
