@@ -18,8 +18,9 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 # Each slice product is exact (32-bit integer sums); an operand carries the
-# rounding of its 32-bit fixed point (2.3e-10 of its range: |factor| <= 1,
-# charges scaled by max |q|) and the ten-product truncation (zero-mean, below
+# rounding of its 32-bit fixed point (2.3e-10 of its range for B, at most
+# twice that for A, whose components round twice: |factor| <= 1, charges
+# scaled by max |q|) and the ten-product truncation (zero-mean, below
 # 1e-9 of the range), so a coefficient of a box of n random-phase particles
 # is off by about sqrt(n) 4e-10: the bound below is relative to the largest
 # coefficient of the box.
