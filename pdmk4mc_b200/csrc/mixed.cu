@@ -362,6 +362,8 @@ __global__ void __launch_bounds__(MixShape<NK>::TTHREADS)
         const double xa = P[a * S::COORD_BOX + off + j];
         const double ca = a == 0 ? it.cx : (a == 1 ? it.cy : it.cz);
         const int Xa = a == 0 ? it.X : (a == 1 ? it.Y : it.Z);
+        // ex: 127 (B); ey: 1; ez: 127 q / max|q| times 2^24, so that A's
+        // fixed point is formed by fix24_dot without a further scaling
         const double scale =
             a == 0 ? SL_SCALE : (a == 1 ? 1.0 : SL_SCALE * 16777216.0 * P[3 * S::COORD_BOX + off + j] * inv_qmax);
         axis_factors_d(xa - ca, it.dk, it.M, Xa, m0, cnt, scale, dst);
